@@ -1,0 +1,416 @@
+#!/usr/bin/env python
+"""bench.py -- sieved integers/s at 1e15 (headline), u64 BPSW tests/s, batched vs plain.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step = the large-offset sieve of [1e15, 1e15 + 2^34) on one GPU with every output of
+that workload (per-2^24-block prime counts, twin counts, 6-tuple counts and checksums,
+maximal gaps with their positions, per-2^20-integer FNV-1a hashes of the prime bitmap).
+Under torchrun each rank sieves its own 2^34-integer range above 1e15 (weak scaling; the
+ranges share nothing, so there is no collective in the data path; NCCL only carries the
+barrier and the max-over-ranks of the device times).
+
+Rank 0 prints one JSON line.  `value` = integers sieved by all ranks / the slowest rank's
+summed device time of the K timed steps (CUDA events on the launching stream; L2 flushed
+with a 256 MiB write between steps, outside the timed events).  `e2e` = the same workload
+through the public host API mp_sieve_range (results copied back to host memory each step),
+timed by the host clock.  The BPSW and plain-form numbers are reported beside it.
+
+--impl reference: the CPU implementation of the same workload on this machine's cores (the
+oracle's restatement of the reference's odd-only sieve, with every output), on a bounded
+sample of the range per step; rank 0 only.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "sieved ints/s @1e15 and u64 BPSW tests/s, batched vs plain; p50/p99 latency"
+LO = 10 ** 15
+SPAN = 1 << 34
+BLOCK_LOG2 = 24
+HASH_LOG2 = 20
+BPSW_SEED, BPSW_COUNT, BPSW_LISTS = 0x3C0FFEE, 1 << 26, 4096
+HBM_FALLBACK_GBS = 6650.0
+WORKLOAD = ("large-offset sieve [1e15, 1e15+2^34) per GPU, odd-only bitmap, sieving primes up to 31623048, "
+            "wheel/pattern presieve 3..89, bucket sieve above the tile; outputs per-2^24-block pi, twins, "
+            "6-tuples {0,4,6,10,12,16} with checksum, max gap + start, per-2^20 FNV-1a bitmap hashes")
+
+
+def peaks_file():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_FALLBACK_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.f = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except Exception:
+                self.p.kill()
+        self.f.flush()
+        rows = []
+        with open(self.f.name) as g:
+            for line in g:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def algorithmic_work(primes, lo, hi, tile_bits):
+    """Exact marks of the sieve (odd multiples m of each sieving prime q >= 97 with
+    max(lo, q^2) <= m < hi + tail) split at the tile size: marks by primes q <= tile_bits are
+    shared-memory atomics, those above are bucket records (4 bytes written + 4 read)."""
+    qi = primes[primes >= 97].astype(np.uint64)
+    top = hi + (1 << 16)
+    start = np.maximum(np.full(len(qi), lo, dtype=np.uint64), qi * qi)
+    # odd multiples of q in [start, top): multiples k q with k odd
+    def count_odd_mult(a, b, q):
+        # number of odd k with a <= k q < b
+        k0 = (a + q - np.uint64(1)) // q
+        k1 = (b + q - np.uint64(1)) // q          # first k with k q >= b
+        odd_below = lambda k: k // np.uint64(2)   # odd numbers < k
+        return (odd_below(k1) - odd_below(k0)).astype(np.float64)
+    m = count_odd_mult(start, np.full(len(qi), top, dtype=np.uint64), qi)
+    small = qi <= np.uint64(tile_bits)
+    return float(m[small].sum()), float(m[~small].sum())
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    import mathpub_b200 as mp
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world != args.gpus and "RANK" in os.environ:
+        pass
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    dev = torch.device("cuda", local)
+    e = mp.Engine(local)
+    L = mp.lib()
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+
+    lo = LO + rank * SPAN
+    hi = lo + SPAN
+    nb = L.mp_sieve_nblocks(lo, hi, BLOCK_LOG2)
+    nh = L.mp_sieve_nhashes(lo, hi, HASH_LOG2)
+    d_out = torch.zeros(8, dtype=torch.int64, device=dev)
+    d_blocks = torch.zeros(nb * 8, dtype=torch.int64, device=dev)
+    d_hash = torch.zeros(nh, dtype=torch.int64, device=dev)
+    import ctypes as C
+    opts = mp.SieveOpts(mp.MODE_BATCHED, 0, BLOCK_LOG2, HASH_LOG2, 0)
+
+    def sieve_dev(o=opts):
+        rc = L.mp_sieve_range_dev(e.handle, lo, hi, C.byref(o), C.c_void_p(d_out.data_ptr()),
+                                  C.c_void_p(d_blocks.data_ptr()), C.c_void_p(d_hash.data_ptr()), None,
+                                  C.c_void_p(sp))
+        if rc != 0:
+            raise mp.MathpubError(rc, L.mp_last_error(e.handle).decode())
+
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+            torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # warm-up (builds the prime tables and captures the graph on the first call)
+    for _ in range(args.warmup):
+        sieve_dev()
+    barrier()
+
+    sampler = ClockSampler(local) if rank == 0 else None
+    if sampler:
+        sampler.start()
+        time.sleep(0.3)
+    barrier()
+    ms = []
+    for _ in range(args.steps):
+        flush.zero_()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        sieve_dev()
+        b.record(stream)
+        b.synchronize()
+        ms.append(a.elapsed_time(b))
+    barrier()
+    clocks = sampler.stop() if sampler else None
+    tot_ms = max_over_ranks(sum(ms))
+    value = world * args.steps * SPAN / (tot_ms / 1e3)
+
+    # results of the timed steps (checked against the fixture when it is present)
+    out = d_out.cpu().numpy().view(np.uint64)
+    res = dict(zip(mp.STATS_FIELDS, [int(x) for x in out]))
+
+    # e2e through the host API: outputs copied to host memory every step
+    e2e_ms = []
+    for _ in range(max(2, min(args.steps, 5))):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e.sieve_range(lo, hi, block_log2=BLOCK_LOG2, hash_log2=HASH_LOG2)
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    e2e_tot = max_over_ranks(statistics.mean(e2e_ms))
+    e2e_value = world * SPAN / (e2e_tot / 1e3)
+    d2h = 64 + nb * 64 + nh * 8
+
+    # profile pass: per-kernel device times on the launching stream
+    e.profile(True)
+    flush.zero_()
+    sieve_dev()
+    torch.cuda.synchronize()
+    prof = e.profile_read()
+    e.profile(False)
+    tile_launches, tile_ms = prof["tile"]
+    scat_launches, scat_ms = prof["scatter"]
+    launches_per_step = sum(v[0] for v in prof.values())
+
+    # plain (per-segment launch) form of the same workload, one step
+    popts = mp.SieveOpts(mp.MODE_PLAIN, 0, BLOCK_LOG2, HASH_LOG2, 0)
+    flush.zero_()
+    torch.cuda.synchronize()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    sieve_dev(popts)
+    b.record(stream)
+    b.synchronize()
+    plain_ms = max_over_ranks(a.elapsed_time(b))
+    plain_out = dict(zip(mp.STATS_FIELDS, [int(x) for x in d_out.cpu().numpy().view(np.uint64)]))
+    plain_value = world * SPAN / (plain_ms / 1e3)
+
+    # BPSW: the seeded 2^26-candidate batch in 4096 uneven lists, device-resident
+    n, lens = mp.bpsw_workload(BPSW_SEED + rank, BPSW_COUNT, BPSW_LISTS)
+    pad = ((lens.astype(np.int64) + 31) // 32) * 32
+    offs = np.concatenate([[0], np.cumsum(pad)]).astype(np.uint64)
+    flat = np.zeros(int(offs[-1]), dtype=np.uint64)
+    src = np.concatenate([[0], np.cumsum(lens.astype(np.int64))])
+    for i in range(len(lens)):
+        flat[int(offs[i]):int(offs[i]) + int(lens[i])] = n[src[i]:src[i + 1]]
+    dn = torch.from_numpy(flat.view(np.int64)).to(dev)
+    db = torch.zeros(int(offs[-1]) // 32, dtype=torch.int32, device=dev)
+
+    def bpsw_dev(mode):
+        rc = L.mp_bpsw_lists_dev(e.handle, C.c_void_p(dn.data_ptr()), C.c_void_p(offs.ctypes.data),
+                                 C.c_void_p(lens.ctypes.data), len(lens), C.c_void_p(db.data_ptr()), mode,
+                                 C.c_void_p(sp))
+        if rc != 0:
+            raise mp.MathpubError(rc, L.mp_last_error(e.handle).decode())
+
+    def time_bpsw(mode, steps):
+        bpsw_dev(mode)
+        torch.cuda.synchronize()
+        tt = []
+        for _ in range(steps):
+            flush.zero_()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            bpsw_dev(mode)
+            b.record(stream)
+            b.synchronize()
+            tt.append(a.elapsed_time(b))
+        return max_over_ranks(statistics.mean(tt))
+
+    bpsw_ms = time_bpsw(mp.MODE_BATCHED, max(3, args.steps))
+    bpsw_bits = db.cpu().numpy().view(np.uint32).copy()
+    bpsw_plain_ms = time_bpsw(mp.MODE_PLAIN, 2)
+    plain_bits = db.cpu().numpy().view(np.uint32)
+    bpsw_same = bool(np.array_equal(bpsw_bits, plain_bits))
+    bpsw_primes = int(np.unpackbits(bpsw_bits.view(np.uint8)).sum())
+
+    peaks = e.probe_peaks()
+    hbm, hbm_src = peaks_file()
+
+    line = None
+    if rank == 0:
+        primes = e.primes_range(3, int(np.sqrt(float(hi + (1 << 16)))) + 2)
+        tile_bits = 1 << 20
+        marks_small, marks_large = algorithmic_work(primes, lo, hi, tile_bits)
+        ntiles = -(-((hi + (1 << 16) - lo) // 2) // tile_bits)
+        tile_bytes = (marks_large * 4 + ntiles * (tile_bits // 8)) / max(tile_launches, 1)
+        tile_avg_s = tile_ms / max(tile_launches, 1) / 1e3
+        achieved = tile_bytes / tile_avg_s / 1e9
+        smem_marks_rate = (marks_small + marks_large) / (tile_ms / 1e3)
+        ref_fixture = None
+        try:
+            with open(os.path.join(ROOT, "tests", "golden", "configs.json")) as f:
+                ref_fixture = json.load(f)["config2"]["stats"]
+        except Exception:
+            pass
+        cpu = cpu_baseline() if world == 1 else None
+        line = {
+            "metric": METRIC, "value": value, "unit": "ints/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": tot_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "lo": lo, "span": SPAN, "block_log2": BLOCK_LOG2,
+                       "hash_log2": HASH_LOG2, "per_rank_range": "[1e15 + r 2^34, 1e15 + (r+1) 2^34)",
+                       "l2": "flushed between steps (256 MiB write outside the timed events)",
+                       "parallelism": f"replicas x{world} (disjoint ranges)"},
+            "e2e": {"value": e2e_value, "unit": "ints/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": d2h,
+                    "api": "mp_sieve_range (host buffers)"},
+            "gpu_launches": launches_per_step * args.steps,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "traffic": None, "kernel": "tile_kernel<20,0>",
+                         "peak_source": f"{hbm_src} (MEASURED_PEAKS.json hbm_gbs)" if hbm_src == "measured" else "fallback",
+                         "algorithmic_bytes_per_launch": tile_bytes, "avg_launch_ms": tile_avg_s * 1e3,
+                         "note": "bytes = bucket records read (4 B per large-prime hit) + bitmap written; "
+                                 "the binding resource is shared-memory atomics, see roofline_smem"},
+            "roofline_smem": {"bound": "smem_atomics", "achieved": smem_marks_rate,
+                              "peak": peaks["smem_atomic_conflict_free"], "unit": "atomic ops/s",
+                              "frac": smem_marks_rate / peaks["smem_atomic_conflict_free"],
+                              "peak_random_addresses": peaks["smem_atomic_random"],
+                              "frac_of_random_peak": smem_marks_rate / peaks["smem_atomic_random"],
+                              "marks_smem": marks_small, "marks_bucket": marks_large,
+                              "peak_source": "measured in this run (mp_probe_peaks)"},
+            "kernels_ms_per_step": {k: v[1] for k, v in prof.items() if v[0]},
+            "plain": {"value": plain_value, "unit": "ints/s", "ms_per_step": plain_ms,
+                      "batched_over_plain": value / plain_value, "same_results": plain_out == res},
+            "bpsw": {"tests_per_s": world * BPSW_COUNT / (bpsw_ms / 1e3), "ms_per_batch": bpsw_ms,
+                     "plain_tests_per_s": world * BPSW_COUNT / (bpsw_plain_ms / 1e3),
+                     "plain_ms_per_batch": bpsw_plain_ms, "batched_over_plain": bpsw_plain_ms / bpsw_ms,
+                     "same_verdicts": bpsw_same, "primes": bpsw_primes,
+                     "workload": "2^26 seeded odd u64 (60% uniform [2^40,2^64), 30% p*q near 2^62, "
+                                 "10% (k+1)(2k+1) / Chernick), 4096 lists, log-uniform lengths"},
+            "probes": peaks,
+            "results": res, "results_match_fixture": (res == ref_fixture) if (ref_fixture and rank == 0 and lo == LO) else None,
+            "clocks": clocks,
+        }
+        if cpu:
+            line["cpu_baseline"] = cpu
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    e.close()
+    if line:
+        print(json.dumps(line), flush=True)
+
+
+def cpu_baseline(sample_log2=31):
+    """The oracle's restatement of the reference's odd-only sieve (every output of the
+    workload) on [1e15, 1e15 + 2^31) with all host threads."""
+    import oracle
+    t = oracle.threads()
+    lo, hi = LO, LO + (1 << sample_log2)
+    t0 = time.perf_counter()
+    oracle.sieve_range(lo, hi, block_log2=BLOCK_LOG2, hash_log2=HASH_LOG2, nthreads=t)
+    dt = time.perf_counter() - t0
+    out = {"value": (hi - lo) / dt, "unit": "ints/s", "cores": t, "kind": "port",
+           "sample": f"[1e15, 1e15+2^{sample_log2}) with every output, {t} threads, {dt:.2f} s"}
+    if oracle.have_ref():
+        t0 = time.perf_counter()
+        oracle.ref_count_sext(lo, hi, t)
+        dt = time.perf_counter() - t0
+        out["reference_sextuplet_count"] = {"value": (hi - lo) / dt, "unit": "ints/s", "kind": "reference",
+                                            "sample": f"a350826 count [1e15, 1e15+2^{sample_log2}), {t} threads "
+                                                      "(6-tuples only: it sieves the admissible classes, not all "
+                                                      "integers)"}
+    return out
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import oracle
+    t = oracle.threads()
+    sample = 1 << 31
+    for _ in range(args.warmup if args.warmup < 2 else 1):
+        oracle.sieve_range(LO, LO + (1 << 26), block_log2=BLOCK_LOG2, hash_log2=HASH_LOG2, nthreads=t)
+    times = []
+    for k in range(args.steps):
+        lo = LO + k * sample
+        t0 = time.perf_counter()
+        oracle.sieve_range(lo, lo + sample, block_log2=BLOCK_LOG2, hash_log2=HASH_LOG2, nthreads=t)
+        times.append(time.perf_counter() - t0)
+    value = sample * len(times) / sum(times)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "ints/s",
+            "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "sample_per_step": "2^31 integers of the range, every output"},
+            "cpu_baseline": {"value": value, "unit": "ints/s", "cores": t, "kind": "port",
+                             "sample": f"[1e15 + k 2^31, +2^31) per step, {t} threads; the reference's "
+                                       "primesieve-based range tools cannot be built here (primesieve is not "
+                                       "vendored), so the oracle's restatement of its odd-only sieve "
+                                       "(A228768/a228768.c:372-415) is timed"},
+            "e2e": {"value": value, "unit": "ints/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

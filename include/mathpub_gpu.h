@@ -1,0 +1,229 @@
+/*
+ * mathpub_gpu.h -- C ABI of the B200 (sm_100a) engine for the integer hot path that the
+ * Mathpub OEIS searches share: the segmented odd-only sieve with its prime-count, twin,
+ * gap and 6-tuple scans; the 64-bit Montgomery BPSW test; and the Fermat quotient
+ * 2^(p-1) mod p^2.
+ *
+ * Conventions (all entry points):
+ *   - plain C types and pointers only; every call returns an int status (MP_OK = 0, or a
+ *     negative MP_E* code) and never calls exit();
+ *   - mp_last_error() gives a message for the last failing call on a handle;
+ *   - a handle owns one CUDA stream, the device-resident sieving-prime tables and scratch
+ *     buffers; calls on one handle are serialised internally, so several host threads may
+ *     share a handle; separate handles run independently;
+ *   - "host" entry points take caller-owned host buffers and copy in and out themselves;
+ *     the *_dev variants take device pointers and a cudaStream_t passed as void* (NULL =
+ *     the handle's stream) and return without synchronising.
+ *
+ * Reference interfaces replaced (paths inside the Mathpub project):
+ *   mp_bpsw_u64 / mp_bpsw_batches   bool bpsw(u128)          A350826/a350826.c:965
+ *                                    (with sprp2_64 :618, slprp64 :766, test_batch64 :1392)
+ *   mp_sieve_range                   the segment sieve + scans of process_class
+ *                                    A350826/a350826.c:1522, tw_run A007508/a007508.c:368,
+ *                                    scan_interval A228768/a228768.c:372, the gap walk of
+ *                                    A000230/a000230.c:38-60, and the primesieve calls
+ *                                    (primesieve_jump_to / next_prime / count_twins) that
+ *                                    e.g. A001220/wieferich.c:1138-1141 makes
+ *   mp_fermat_q_base2                u64 fermat_quotient(u64 p, int j, u128 *res)
+ *                                    A001220/wieferich.c:939
+ *   mp_wieferich_range               scan_chunk + process_batch + finish_lanes
+ *                                    A001220/wieferich.c:1129, :1086, :1051
+ *   the int-status / caller-owned-buffer style follows the reference's own C/CUDA split,
+ *   gapchain/gapsieve_cuda.h:1-70.
+ */
+#ifndef MATHPUB_GPU_H
+#define MATHPUB_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define MP_OK         0
+#define MP_EINVAL    -1   /* bad argument (range, size, null pointer)            */
+#define MP_ENOMEM    -2   /* device or host allocation failed                     */
+#define MP_ECUDA     -3   /* CUDA runtime error                                   */
+#define MP_ETIMEOUT  -4   /* a bounded device wait gave up (error flag set)       */
+#define MP_EOVERFLOW -5   /* a device buffer bound was exceeded (retry failed)    */
+#define MP_ERANGE    -6   /* outside the supported range (e.g. hi > 2^64 - 2^18)  */
+#define MP_EAGAIN    -7   /* serving: result not ready yet                        */
+#define MP_EBUSY     -8   /* serving: queue full / not enough free device memory  */
+
+typedef struct mp_handle mp_handle;
+
+/* ---- handle ---- */
+int mp_init(int device, mp_handle **out);
+int mp_free(mp_handle *h);
+const char *mp_last_error(const mp_handle *h);
+int mp_version(void);                       /* 100 * major + minor */
+/* last device time of the main kernels of the previous call, in milliseconds (CUDA events
+   on the handle's stream around the launches; 0 if not timed) */
+double mp_last_kernel_ms(const mp_handle *h);
+
+/* ---- sieve ----
+ * Odd-only bitmap: base = lo & ~1, bit i <-> the odd number base + 2i + 1, bit = 1 for a
+ * prime; in-range bits i < (hi - base) / 2.  Outputs:
+ *   pi        number of primes p in [lo, hi) (2 included when lo <= 2 < hi)
+ *   twins     number of p in [lo, hi) with p + 2 prime
+ *   max_gap   max over primes p in [lo, hi) of nextprime(p) - p (the next prime may lie
+ *             beyond hi), gap_start = the smallest p attaining it; 0, 0 without primes
+ *   tuple6    number of p in [lo, hi) with p + {0, 4, 6, 10, 12, 16} all prime (members may
+ *             lie beyond hi); tuple6_cks = sum of mix64(p) mod 2^64 (splitmix64 finaliser,
+ *             A350826/a350826.c:425-438), the reference's order-free checksum
+ *   first_prime / last_prime   first and last prime in [lo, hi) (0 if none)
+ * Blocks: block b = [lo + b 2^block_log2, lo + (b+1) 2^block_log2) intersected with
+ * [lo, hi), nblocks = ceil((hi - lo) / 2^block_log2), with the same fields per block.
+ * Hashes: FNV-1a-64 per hash segment of 2^hash_log2 integers = 2^(hash_log2 - 1) bits,
+ * over ceil(len/8) bytes (bit j of byte k = bit 8k + j of the segment), nseg =
+ * ceil(nbits / 2^(hash_log2 - 1)).
+ * Bitmap: ceil(nbits / 64) little-endian u64 words, bits beyond the range zero.
+ * Limits: lo < hi <= 2^64 - 2^18.
+ */
+typedef struct {
+    uint64_t pi, twins, max_gap, gap_start, tuple6, tuple6_cks, first_prime, last_prime;
+} mp_range_stats;
+
+typedef mp_range_stats mp_block_stats;
+
+#define MP_MODE_BATCHED 0   /* persistent tile kernel + device work queue + CUDA graph */
+#define MP_MODE_PLAIN   1   /* one launch per segment (the reference's per-segment loop) */
+
+typedef struct {
+    uint32_t mode;          /* MP_MODE_BATCHED (default) or MP_MODE_PLAIN */
+    uint32_t tile_log2;     /* bits per tile: 0 = autotuned, else 18, 19 or 20 */
+    uint32_t block_log2;    /* per-block stats width (integers); 0 = none; else >= tile_log2+1 */
+    uint32_t hash_log2;     /* hash segment width (integers); 0 = no hashes; else 4..40 */
+    uint32_t threads;       /* threads per CTA: 0 = autotuned, else 256, 512 or 1024 */
+    uint32_t reserved[3];
+} mp_sieve_opts;
+
+/* number of blocks / hash segments / bitmap words that mp_sieve_range fills for [lo, hi) */
+uint64_t mp_sieve_nblocks(uint64_t lo, uint64_t hi, uint32_t block_log2);
+uint64_t mp_sieve_nhashes(uint64_t lo, uint64_t hi, uint32_t hash_log2);
+uint64_t mp_sieve_nwords(uint64_t lo, uint64_t hi);
+
+int mp_sieve_range(mp_handle *h, uint64_t lo, uint64_t hi, const mp_sieve_opts *opts,
+                   mp_range_stats *out, mp_block_stats *blocks /* nullable */,
+                   uint64_t *seg_hash /* nullable */, uint64_t *bitmap /* nullable */);
+
+/* same with device output buffers (each nullable except d_out) on `stream` (NULL = the
+   handle's stream); returns once the work is queued */
+int mp_sieve_range_dev(mp_handle *h, uint64_t lo, uint64_t hi, const mp_sieve_opts *opts,
+                       mp_range_stats *d_out, mp_block_stats *d_blocks, uint64_t *d_hash,
+                       uint64_t *d_bitmap, void *stream);
+
+/* all primes in [lo, hi) in increasing order into a host array of cap entries; *count =
+   the number of primes (only min(count, cap) are written) */
+int mp_primes_range(mp_handle *h, uint64_t lo, uint64_t hi, uint64_t *primes, size_t cap,
+                    size_t *count);
+
+/* ---- BPSW ----
+ * verdict bit i (bit i & 7 of byte i >> 3) = 1 iff n[i] is prime.  For n < 2^64 this is
+ * BPSW (base-2 strong test + strong Lucas test with Selfridge's parameters) after trial
+ * division; there is no BPSW pseudoprime below 2^64, so the verdict is exact.
+ */
+int mp_bpsw_u64(mp_handle *h, const uint64_t *n, size_t count, uint8_t *verdict_bits);
+
+/* many candidate lists of uneven length in one batched call: out[i] receives
+   ceil(lens[i] / 8) bytes of verdict bits for lists[i] */
+int mp_bpsw_batches(mp_handle *h, const uint64_t *const *lists, const uint32_t *lens,
+                    uint32_t nlists, uint8_t *const *out);
+
+/* device form: candidates laid out as nlists lists, list i at d_n + offs[i] (offs[i] a
+   multiple of 32, host array offs[0..nlists]), verdict words (u32, bit i & 31 of word
+   i >> 5) at d_bits + offs[i] / 32; mode MP_MODE_BATCHED (one persistent launch) or
+   MP_MODE_PLAIN (one launch per list) */
+int mp_bpsw_lists_dev(mp_handle *h, const uint64_t *d_n, const uint64_t *offs,
+                      const uint32_t *lens, uint32_t nlists, uint32_t *d_bits, uint32_t mode,
+                      void *stream);
+
+/* ---- Fermat quotient, base 2 ----
+ * q = (2^(p-1) mod p^2 - 1) / p for odd primes 3 <= p < 2^63 (A001220/wieferich.c:939);
+ * for p = 2 or an even p the entry is 0.  A result that fails Fermat's little theorem
+ * (q >= p: a wrong residue) is returned as UINT64_MAX and counted as an error.
+ */
+int mp_fermat_q_base2(mp_handle *h, const uint64_t *p, size_t count, uint64_t *q_out);
+int mp_fermat_q_base2_dev(mp_handle *h, const uint64_t *d_p, size_t count, uint64_t *d_q,
+                          void *stream);
+
+/* every prime p in [lo, hi), hi <= 2^63, found by the GPU sieve; per p >= 3: q as above,
+ *   primes        number of primes in [lo, hi) (2 included)
+ *   tests         number of quotients computed (p >= 3)
+ *   near          number of p with 1000 |A| < p, A = the symmetric residue of q
+ *                 (A001220/wieferich.c:1068)
+ *   flt           number of results failing q < p (0 unless the device is faulty)
+ *   cks           sum of mix64(q ^ (p * 0x9E3779B97F4A7C15)) mod 2^64 (the reference's
+ *                 checksum, A001220/wieferich.c:1064)
+ *   ordered_hash  H <- H * 0x100000001b3 + mix64(p ^ mix64(q)) (mod 2^64) in p order
+ *   hits          the Wieferich primes (q = 0) found, nhits of them (first 16 stored) */
+typedef struct {
+    uint64_t primes, tests, near, flt, cks, ordered_hash, nhits;
+    uint64_t hits[16];
+} mp_wief_stats;
+
+int mp_wieferich_range(mp_handle *h, uint64_t lo, uint64_t hi, mp_wief_stats *out);
+
+/* ---- autotuner ----
+ * Times the sieve tile geometry (tile bits x threads) on a short range at height `lo`
+ * and the Fermat kernel variants, and keeps the fastest per handle.  Called implicitly
+ * (on a small range) by the first call that needs it; call it explicitly to tune for a
+ * given height.  *report receives a short text summary (nullable, cap bytes). */
+int mp_autotune(mp_handle *h, uint64_t lo, char *report, size_t cap);
+
+/* ---- measurement ----
+ * mp_profile_enable(h, 1) brackets every launch of the timed kernels with CUDA events on the
+ * stream it runs on (batched sieve calls then run directly instead of replaying a captured
+ * graph); mp_profile_read fills, for the categories "scatter, tile, fold, hash, bpsw_batched,
+ * bpsw_plain, fermat, fermat_stats" in that order, the launch counts and summed device
+ * milliseconds since the previous read.
+ * mp_probe_peaks measures device-wide rates (operations per second): shared-memory atomicOr
+ * with the lanes of a warp on distinct banks and on random words, and 32-bit integer
+ * multiply-adds.  These are the roofline denominators of the sieve and the Montgomery kernels.
+ */
+int mp_profile_enable(mp_handle *h, int on);
+int mp_profile_read(mp_handle *h, uint64_t *launches, double *ms, int ncat);
+int mp_probe_peaks(mp_handle *h, double *smem_atomic_conflict_free, double *smem_atomic_random,
+                   double *imad32);
+
+/* ---- serving (continuous batching) ----
+ * Requests of two kinds: range queries [lo, hi) -> pi, max gap (+ start), twins; and
+ * primality batches of up to 65536 candidates -> verdict bits.  Requests are admitted
+ * while device memory (a budget) and in-flight slots allow; admitted work is cut into
+ * tiles and candidate slices that share the device with other requests' work.  Each
+ * result is identical to the same request run alone.
+ */
+typedef struct mp_server mp_server;
+
+typedef struct {
+    uint64_t mem_budget;    /* bytes of device memory for in-flight requests (0 = auto) */
+    uint32_t max_inflight;  /* requests admitted at once (0 = 256) */
+    uint32_t streams;       /* device streams that overlap batches (0 = 4) */
+    uint64_t prime_limit;   /* resident sieving primes up to this bound (0 = 2^32 - 1) */
+} mp_serve_opts;
+
+typedef struct {
+    uint32_t kind;          /* 1 = range, 2 = primality */
+    int32_t status;         /* MP_OK or an error code */
+    uint64_t pi, max_gap, gap_start, twins;     /* range results */
+    uint32_t count;         /* primality: number of candidates */
+    double submit_s, done_s;                    /* host clock (seconds) at submit / completion */
+} mp_serve_result;
+
+int mp_serve_open(mp_handle *h, const mp_serve_opts *opts, mp_server **out);
+int mp_serve_submit_range(mp_server *s, uint64_t lo, uint64_t hi, uint64_t *req_id);
+/* the candidates are copied at submit; verdict bits go to `verdict_bits` (caller-owned,
+   ceil(count/8) bytes, valid once poll reports the request done) */
+int mp_serve_submit_bpsw(mp_server *s, const uint64_t *n, uint32_t count,
+                         uint8_t *verdict_bits, uint64_t *req_id);
+/* MP_OK and *res filled when done (the request is then retired), MP_EAGAIN if pending;
+   waits up to wait_ms milliseconds */
+int mp_serve_poll(mp_server *s, uint64_t req_id, mp_serve_result *res, int wait_ms);
+int mp_serve_close(mp_server *s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,339 @@
+// mp_bpsw.cu -- 64-bit Montgomery BPSW primality test for B200 (sm_100a).
+//
+// Reference (paths inside the Mathpub project): inv64/mmul64/madd64/msub64/mhalf64
+// A350826/a350826.c:565-604, sprp2_64 :618-638, jacobi :693, selfridge :739, slprp64
+// :766-799, bpsw :965-969, and the breadth-first batching of test_batch64 :1392.
+//
+// Differences in method, not in results:
+//   - R mod n (the Montgomery form of 1) is computed by doubling 2^(bitlen(n)-1) up to 2^64
+//     (exact; no division and no floating-point estimate), and the forms of Q and D by
+//     double-and-add of that one;
+//   - trial division by the odd primes up to 127 uses the multiplicative-inverse test
+//     (q | n iff n * q^-1 mod 2^64 <= (2^64 - 1) / q, for odd q) before any exponentiation;
+//   - perfect squares are rejected with an exact integer square root.
+// The verdict is primality for every n < 2^64 (BPSW has no pseudoprime below 2^64).
+//
+// Two launch structures:
+//   plain    one launch per candidate list, one thread per candidate, all phases inline;
+//   batched  one persistent launch over every list: CTAs pop chunks of 2048 candidates from
+//            a device work queue, trial-divide, compact the survivors in shared memory, run
+//            the base-2 test on them, compact the passers, run the Lucas test, and write the
+//            verdict words.  Compaction keeps the warps' lanes on uniform work.
+#include "mp_common.cuh"
+
+#define TD_N 30            // odd primes 3..127
+#define BPSW_CHUNK 2048
+
+__constant__ u64 c_td_inv[TD_N];
+__constant__ u64 c_td_lim[TD_N];
+__constant__ u64 c_small_prime_mask[2];   // bit n set iff n < 128 is prime
+
+// ---- 64-bit Montgomery arithmetic, R = 2^64 ----
+
+__device__ __forceinline__ u64 m_mul(u64 a, u64 b, u64 n, u64 ni)
+{
+    const u64 tl = a * b, th = __umul64hi(a, b);
+    const u64 m = tl * ni;
+    const u64 mh = __umul64hi(m, n);
+    const u64 r = th - mh;
+    return th < mh ? r + n : r;
+}
+__device__ __forceinline__ u64 m_add(u64 a, u64 b, u64 n) { const u64 s = a + b; return (s < a || s >= n) ? s - n : s; }
+__device__ __forceinline__ u64 m_sub(u64 a, u64 b, u64 n) { return a >= b ? a - b : a - b + n; }
+__device__ __forceinline__ u64 m_half(u64 a, u64 n) { return (a & 1) ? (a >> 1) + (n >> 1) + 1 : a >> 1; }
+
+// n^-1 mod 2^64 for odd n: (3n) xor 2 is correct to 5 bits; four Newton steps give 80
+__device__ __forceinline__ u64 m_inv(u64 n)
+{
+    u64 x = (3 * n) ^ 2;
+    x *= 2 - n * x;
+    x *= 2 - n * x;
+    x *= 2 - n * x;
+    x *= 2 - n * x;
+    return x;
+}
+
+// 2^64 mod n for odd n > 1, by doubling 2^b (b = top bit of n, so 2^b < n) 64 - b times
+__device__ __forceinline__ u64 m_one(u64 n)
+{
+    const int b = 63 - __clzll((long long)n);
+    u64 x = 1ull << b;
+    for (int i = b; i < 64; i++) x = m_add(x, x, n);
+    return x;
+}
+
+// Montgomery form of a small signed integer v (|v| < n) by double-and-add of `one`
+__device__ __forceinline__ u64 m_small(i32 v, u64 one, u64 n)
+{
+    u32 a = v < 0 ? (u32)(-v) : (u32)v;
+    u64 r = 0;
+    for (int i = 31 - __clz((int)(a | 1)); i >= 0; i--) {
+        r = m_add(r, r, n);
+        if ((a >> i) & 1) r = m_add(r, one, n);
+    }
+    if (v < 0 && r) r = n - r;
+    return r;
+}
+
+// ---- trial division ----
+// 1 = prime, 0 = composite, -1 = undecided (odd, no factor <= 127, n >= 131^2)
+__device__ __forceinline__ int td_verdict(u64 n)
+{
+    if (n < 128) return (int)((c_small_prime_mask[n >> 6] >> (n & 63)) & 1);
+    if (!(n & 1)) return 0;
+#pragma unroll
+    for (int k = 0; k < TD_N; k++)
+        if (n * c_td_inv[k] <= c_td_lim[k]) return 0;
+    if (n < 131ull * 131ull) return 1;
+    return -1;
+}
+
+// ---- base-2 strong probable-prime test (odd n > 2) ----
+__device__ __forceinline__ bool sprp2_dev(u64 n, u64 ni, u64 one)
+{
+    const u64 mone = n - one;
+    u64 d = n - 1;
+    const int s = __ffsll((long long)d) - 1;
+    d >>= s;
+    const int top = 63 - __clzll((long long)d);
+    u64 x = m_add(one, one, n);                  // 2, for the top bit of d
+    for (int i = top - 1; i >= 0; i--) {
+        x = m_mul(x, x, n, ni);
+        const u64 y = m_add(x, x, n);
+        x = ((d >> i) & 1) ? y : x;
+    }
+    if (x == one || x == mone) return true;
+    for (int i = 1; i < s; i++) {
+        x = m_mul(x, x, n, ni);
+        if (x == mone) return true;
+        if (x == one) return false;
+    }
+    return false;
+}
+
+// ---- strong Lucas test ----
+
+// Jacobi symbol (D/n) for odd D with |D| < n, odd n
+__device__ __forceinline__ int jacobi_small(i32 D, u64 n)
+{
+    int t = 1;
+    u32 a;
+    if (D < 0) {
+        a = (u32)(-D);
+        if ((n & 3) == 3) t = -t;             // (-1/n)
+    } else a = (u32)D;
+    if ((a & 3) == 3 && (n & 3) == 3) t = -t; // reciprocity (a/n) = +-(n/a), a odd
+    u32 x = (u32)(n % a), m = a;
+    while (x) {
+        while (!(x & 1)) {
+            x >>= 1;
+            const u32 r = m & 7;
+            if (r == 3 || r == 5) t = -t;
+        }
+        const u32 tmp = x; x = m; m = tmp;
+        if ((x & 3) == 3 && (m & 3) == 3) t = -t;
+        x %= m;
+    }
+    return m == 1 ? t : 0;
+}
+
+__device__ __forceinline__ u64 isqrt_dev(u64 n)
+{
+    u64 r = 0, bit = 1ull << 62;
+    while (bit > n) bit >>= 2;
+    while (bit) {
+        if (n >= r + bit) { n -= r + bit; r = (r >> 1) + bit; }
+        else r >>= 1;
+        bit >>= 2;
+    }
+    return r;
+}
+
+__device__ __forceinline__ bool is_square_dev(u64 n)
+{
+    // squares mod 64 are 0, 1, 4, 9, 16, 17, 25, 33, 36, 41, 49, 57
+    const u64 sq64 = (1ull << 0) | (1ull << 1) | (1ull << 4) | (1ull << 9) | (1ull << 16) | (1ull << 17) |
+                     (1ull << 25) | (1ull << 33) | (1ull << 36) | (1ull << 41) | (1ull << 49) | (1ull << 57);
+    if (!((sq64 >> (n & 63)) & 1)) return false;
+    const u64 r = isqrt_dev(n);
+    return r * r == n;
+}
+
+// Selfridge method A: first D in 5, -7, 9, -11, ... with (D/n) = -1.  The search is bounded;
+// for n < 2^64 that is not a square a suitable D has |D| far below the bound.
+__device__ __forceinline__ bool selfridge_dev(u64 n, i32 *Dout)
+{
+    if (is_square_dev(n)) return false;
+    i32 D = 5;
+    for (int it = 0; it < 4096; it++) {
+        const int j = jacobi_small(D, n);
+        if (j == -1) { *Dout = D; return true; }
+        if (j == 0 && (u64)(D < 0 ? -D : D) != n) return false;
+        D = D > 0 ? -(D + 2) : -(D - 2);
+    }
+    return false;
+}
+
+__device__ __forceinline__ bool slprp_dev(u64 n, u64 ni, u64 one)
+{
+    i32 D;
+    if (!selfridge_dev(n, &D)) return false;
+    const i32 Q = (1 - D) / 4;
+    const u64 Qm = m_small(Q, one, n), Dm = m_small(D, one, n);
+    u64 d = n + 1;                               // n < 2^64 - 1 here (2^64 - 1 has factor 3)
+    const int s = __ffsll((long long)d) - 1;
+    d >>= s;
+    u64 U = one, V = one, Qk = Qm;
+    for (int b = 62 - __clzll((long long)d); b >= 0; b--) {
+        U = m_mul(U, V, n, ni);
+        V = m_sub(m_mul(V, V, n, ni), m_add(Qk, Qk, n), n);
+        Qk = m_mul(Qk, Qk, n, ni);
+        if ((d >> b) & 1) {
+            const u64 U2 = m_add(U, V, n);
+            const u64 V2 = m_add(m_mul(Dm, U, n, ni), V, n);
+            U = m_half(U2, n);
+            V = m_half(V2, n);
+            Qk = m_mul(Qk, Qm, n, ni);
+        }
+    }
+    if (U == 0 || V == 0) return true;
+    for (int r = 1; r < s; r++) {
+        V = m_sub(m_mul(V, V, n, ni), m_add(Qk, Qk, n), n);
+        if (V == 0) return true;
+        Qk = m_mul(Qk, Qk, n, ni);
+    }
+    return false;
+}
+
+__device__ __forceinline__ bool bpsw_full(u64 n)
+{
+    const int v = td_verdict(n);
+    if (v >= 0) return v != 0;
+    const u64 ni = m_inv(n), one = m_one(n);
+    return sprp2_dev(n, ni, one) && slprp_dev(n, ni, one);
+}
+
+// ---- plain form: one thread per candidate of one list ----
+__global__ void __launch_bounds__(256) bpsw_plain_kernel(const u64 *__restrict__ n, u32 len, u32 *__restrict__ bits)
+{
+    const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    bool v = false;
+    if (i < len) v = bpsw_full(__ldg(n + i));
+    const u32 b = __ballot_sync(0xffffffffu, v);
+    if ((threadIdx.x & 31) == 0 && i < len) bits[i >> 5] = b;
+}
+
+// ---- batched form: persistent CTAs over chunks of the concatenated lists ----
+__global__ void __launch_bounds__(256) bpsw_batched_kernel(const u64 *__restrict__ n, u64 total,
+                                                            u32 *__restrict__ bits, u32 *queue)
+{
+    __shared__ u64 s_n[BPSW_CHUNK];
+    __shared__ u16 s_idx[BPSW_CHUNK];
+    __shared__ u16 s_idx2[BPSW_CHUNK];
+    __shared__ u32 s_bits[BPSW_CHUNK / 32];
+    __shared__ u32 s_cnt[2];
+    __shared__ u32 s_chunk;
+    const u32 tid = threadIdx.x, nth = blockDim.x;
+    const u64 nchunks = (total + BPSW_CHUNK - 1) / BPSW_CHUNK;
+    for (;;) {
+        if (tid == 0) {
+            s_chunk = atomicAdd(queue, 1u);
+            s_cnt[0] = s_cnt[1] = 0;
+        }
+        for (u32 w = tid; w < BPSW_CHUNK / 32; w += nth) s_bits[w] = 0;
+        __syncthreads();
+        const u32 c = s_chunk;
+        if (c >= nchunks) break;
+        const u64 c0 = (u64)c * BPSW_CHUNK;
+        const u32 len = (u32)(total - c0 < BPSW_CHUNK ? total - c0 : BPSW_CHUNK);
+        // 1. trial division; undecided candidates are compacted
+        for (u32 i = tid; i < len; i += nth) {
+            const u64 x = __ldg(n + c0 + i);
+            s_n[i] = x;
+            const int v = td_verdict(x);
+            if (v == 1) atomicOr(&s_bits[i >> 5], 1u << (i & 31));
+            else if (v < 0) s_idx[atomicAdd(&s_cnt[0], 1u)] = (u16)i;
+        }
+        __syncthreads();
+        // 2. base-2 strong test on the survivors; passers are compacted
+        const u32 ns = s_cnt[0];
+        for (u32 k = tid; k < ns; k += nth) {
+            const u32 i = s_idx[k];
+            const u64 x = s_n[i];
+            if (sprp2_dev(x, m_inv(x), m_one(x))) s_idx2[atomicAdd(&s_cnt[1], 1u)] = (u16)i;
+        }
+        __syncthreads();
+        // 3. strong Lucas test on the base-2 passers
+        const u32 nl = s_cnt[1];
+        for (u32 k = tid; k < nl; k += nth) {
+            const u32 i = s_idx2[k];
+            const u64 x = s_n[i];
+            if (slprp_dev(x, m_inv(x), m_one(x))) atomicOr(&s_bits[i >> 5], 1u << (i & 31));
+        }
+        __syncthreads();
+        const u32 nw = (len + 31) / 32;
+        for (u32 w = tid; w < nw; w += nth) bits[(c0 >> 5) + w] = s_bits[w];
+        __syncthreads();
+    }
+}
+
+// ---- host side ----
+
+static bool g_bpsw_consts[16] = {false};
+
+static int bpsw_consts(mp_handle *h)
+{
+    if (h->device >= 0 && h->device < 16 && g_bpsw_consts[h->device]) return MP_OK;
+    static const u32 tdp[TD_N] = {3,  5,  7,  11, 13, 17, 19, 23, 29, 31, 37, 41,  43,  47,  53,
+                                  59, 61, 67, 71, 73, 79, 83, 89, 97, 101, 103, 107, 109, 113, 127};
+    u64 inv[TD_N], lim[TD_N], mask[2] = {0, 0};
+    for (int k = 0; k < TD_N; k++) {
+        const u64 q = tdp[k];
+        u64 x = (3 * q) ^ 2;
+        for (int i = 0; i < 4; i++) x *= 2 - q * x;
+        inv[k] = x;
+        lim[k] = ~0ull / q;
+    }
+    for (u32 v = 2; v < 128; v++) {
+        bool p = true;
+        for (u32 d = 2; d * d <= v; d++) if (v % d == 0) { p = false; break; }
+        if (p) mask[v >> 6] |= 1ull << (v & 63);
+    }
+    MP_CUDA(h, cudaMemcpyToSymbol(c_td_inv, inv, sizeof inv));
+    MP_CUDA(h, cudaMemcpyToSymbol(c_td_lim, lim, sizeof lim));
+    MP_CUDA(h, cudaMemcpyToSymbol(c_small_prime_mask, mask, sizeof mask));
+    if (h->device >= 0 && h->device < 16) g_bpsw_consts[h->device] = true;
+    return MP_OK;
+}
+
+// lists at d_n + offs[i] (offs multiples of 32, host array of nlists + 1 entries), verdict
+// words at d_bits + offs[i] / 32
+int mp_bpsw_run(mp_handle *h, const u64 *d_n, const u64 *offs, const u32 *lens, u32 nlists, u32 *d_bits,
+                u32 mode, cudaStream_t st)
+{
+    MP_TRY(bpsw_consts(h));
+    if (mode == MP_MODE_PLAIN) {
+        for (u32 i = 0; i < nlists; i++) {
+            if (!lens[i]) continue;
+            if (offs[i] & 31) return mp_set_error(h, MP_EINVAL, "list offsets must be multiples of 32");
+            ProfScope ps(h, PROF_BPSW_PLAIN, st);
+            bpsw_plain_kernel<<<(lens[i] + 255) / 256, 256, 0, st>>>(d_n + offs[i], lens[i], d_bits + offs[i] / 32);
+            MP_CUDA(h, cudaGetLastError());
+        }
+        return MP_OK;
+    }
+    const u64 total = offs[nlists];
+    if (!total) return MP_OK;
+    MP_CUDA(h, h->queue.ensure(64));
+    MP_CUDA(h, cudaMemsetAsync(h->queue.p, 0, 4, st));
+    int per_sm = 0;
+    MP_CUDA(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bpsw_batched_kernel, 256, 0));
+    if (per_sm < 1) per_sm = 1;
+    u64 grid = (u64)h->sm_count * per_sm;
+    const u64 nchunks = (total + BPSW_CHUNK - 1) / BPSW_CHUNK;
+    if (grid > nchunks) grid = nchunks;
+    ProfScope ps(h, PROF_BPSW_BATCHED, st);
+    bpsw_batched_kernel<<<(unsigned)grid, 256, 0, st>>>(d_n, total, d_bits, h->queue.as<u32>());
+    MP_CUDA(h, cudaGetLastError());
+    return MP_OK;
+}

@@ -1,0 +1,281 @@
+// mp_fermat.cu -- Fermat quotients q_p(2) = (2^(p-1) mod p^2 - 1) / p on B200 (sm_100a).
+//
+// Reference (paths inside the Mathpub project): pctx_init / msqr / redc
+// A001220/wieferich.c:546-645 (Montgomery arithmetic mod N = p^2 with R = 2^128, p^-1 by
+// Newton from (3p) xor 2), fermat_quotient :939 (q = (r - 1) p^-1 mod 2^64), finish_lanes
+// :1051-1075 (Fermat's little theorem check q < p, checksum mix64(q ^ p * GOLD), symmetric
+// residue A).
+//
+// The device form keeps the same mathematics with a different number layout: N = p^2 is
+// held in K 32-bit limbs (K = 3, R = 2^96, for p < 2^47; K = 4, R = 2^128, for p < 2^63),
+// multiplied with the CIOS Montgomery product on 32x32->64 integer multiply-adds.  The form
+// of 1 (R mod N) is found by doubling 2^(bitlen(N)-1) up to R, exactly; the reference's
+// double-precision quotient estimates are not used.  The exponent p - 1 is processed left
+// to right: square, then double when the bit is 1 (base 2 needs no multiplier table).
+#include "mp_common.cuh"
+
+template <int K>
+__device__ __forceinline__ void cond_sub(u32 (&t)[K], u32 top, const u32 (&n)[K])
+{
+    // t (with carry word `top`) < 2N: subtract N once if t >= N
+    u32 d[K];
+    u64 borrow = 0;
+#pragma unroll
+    for (int j = 0; j < K; j++) {
+        const u64 s = (u64)t[j] - n[j] - borrow;
+        d[j] = (u32)s;
+        borrow = (s >> 63) & 1;
+    }
+    const bool ge = top || !borrow;
+#pragma unroll
+    for (int j = 0; j < K; j++) t[j] = ge ? d[j] : t[j];
+}
+
+// r = a * b / R mod N (a, b < N), CIOS with 32-bit limbs
+template <int K>
+__device__ __forceinline__ void mmul(u32 (&r)[K], const u32 (&a)[K], const u32 (&b)[K], const u32 (&n)[K], u32 np)
+{
+    u32 t[K + 2];
+#pragma unroll
+    for (int j = 0; j < K + 2; j++) t[j] = 0;
+#pragma unroll
+    for (int i = 0; i < K; i++) {
+        u64 C = 0;
+#pragma unroll
+        for (int j = 0; j < K; j++) {
+            const u64 s = (u64)t[j] + (u64)a[j] * b[i] + C;
+            t[j] = (u32)s;
+            C = s >> 32;
+        }
+        u64 s = (u64)t[K] + C;
+        t[K] = (u32)s;
+        t[K + 1] = (u32)(s >> 32);
+        const u32 m = t[0] * np;
+        s = (u64)t[0] + (u64)m * n[0];
+        C = s >> 32;
+#pragma unroll
+        for (int j = 1; j < K; j++) {
+            s = (u64)t[j] + (u64)m * n[j] + C;
+            t[j - 1] = (u32)s;
+            C = s >> 32;
+        }
+        s = (u64)t[K] + C;
+        t[K - 1] = (u32)s;
+        t[K] = t[K + 1] + (u32)(s >> 32);
+    }
+    u32 o[K];
+#pragma unroll
+    for (int j = 0; j < K; j++) o[j] = t[j];
+    cond_sub<K>(o, t[K], n);
+#pragma unroll
+    for (int j = 0; j < K; j++) r[j] = o[j];
+}
+
+// x = 2x mod N (x < N, 2N < R)
+template <int K>
+__device__ __forceinline__ void mdbl(u32 (&x)[K], const u32 (&n)[K])
+{
+    u32 y[K];
+    y[0] = x[0] << 1;
+#pragma unroll
+    for (int j = 1; j < K; j++) y[j] = (x[j] << 1) | (x[j - 1] >> 31);
+    cond_sub<K>(y, 0u, n);
+#pragma unroll
+    for (int j = 0; j < K; j++) x[j] = y[j];
+}
+
+struct FermOut { u64 q; bool ok; };
+
+// q_p(2) for odd p >= 3 (p < 2^47 for K = 3, p < 2^63 for K = 4)
+template <int K>
+__device__ __forceinline__ FermOut fermat_one(u64 p)
+{
+    u64 pinv = (3 * p) ^ 2;
+    pinv *= 2 - p * pinv;
+    pinv *= 2 - p * pinv;
+    pinv *= 2 - p * pinv;
+    pinv *= 2 - p * pinv;
+    const u32 np = 0u - (u32)(pinv * pinv);            // -N^-1 mod 2^32
+    const u64 N0 = p * p, N1 = __umul64hi(p, p);
+    u32 n[K];
+    n[0] = (u32)N0; n[1] = (u32)(N0 >> 32); n[2] = (u32)N1;
+    if (K == 4) n[K - 1] = (u32)(N1 >> 32);
+    // one = R mod N: start at 2^(top bit of N), double up to 2^(32K)
+    const int topbit = N1 ? 64 + 63 - __clzll((long long)N1) : 63 - __clzll((long long)N0);
+    u32 x[K];
+#pragma unroll
+    for (int j = 0; j < K; j++) x[j] = (topbit >> 5) == j ? (1u << (topbit & 31)) : 0u;
+    for (int i = topbit; i < 32 * K; i++) mdbl<K>(x, n);
+    // left-to-right binary exponentiation of 2 to e = p - 1; leading zero bits keep x = 1
+    const u64 e = p - 1;
+    for (int b = 63 - __clzll((long long)e); b >= 0; b--) {
+        mmul<K>(x, x, x, n, np);
+        u32 y[K];
+#pragma unroll
+        for (int j = 0; j < K; j++) y[j] = x[j];
+        mdbl<K>(y, n);
+        const bool bit = (e >> b) & 1;
+#pragma unroll
+        for (int j = 0; j < K; j++) x[j] = bit ? y[j] : x[j];
+    }
+    // leave Montgomery form: multiply by 1
+    u32 one[K];
+#pragma unroll
+    for (int j = 0; j < K; j++) one[j] = j == 0 ? 1u : 0u;
+    mmul<K>(x, x, one, n, np);
+    const u64 r = (u64)x[0] | ((u64)x[1] << 32);
+    FermOut o;
+    o.q = (r - 1) * pinv;
+    o.ok = o.q < p;
+    return o;
+}
+
+// one prime per thread (ILP = 1) or two interleaved primes per thread (ILP = 2)
+template <int K, int ILP>
+__global__ void __launch_bounds__(256) fermat_kernel(const u64 *__restrict__ P, u64 count, u64 *__restrict__ Q)
+{
+    const u64 stride = (u64)gridDim.x * blockDim.x * ILP;
+    for (u64 i = ((u64)blockIdx.x * blockDim.x + threadIdx.x) * ILP; i < count; i += stride) {
+        if (ILP == 1) {
+            const u64 p = __ldg(P + i);
+            u64 q = 0;
+            if (p >= 3 && (p & 1)) { const FermOut o = fermat_one<K>(p); q = o.ok ? o.q : ~0ull; }
+            Q[i] = q;
+        } else {
+            const u64 p0 = __ldg(P + i), p1 = i + 1 < count ? __ldg(P + i + 1) : 3;
+            const bool v0 = p0 >= 3 && (p0 & 1), v1 = p1 >= 3 && (p1 & 1);
+            const FermOut o0 = fermat_one<K>(v0 ? p0 : 3), o1 = fermat_one<K>(v1 ? p1 : 3);
+            Q[i] = v0 ? (o0.ok ? o0.q : ~0ull) : 0;
+            if (i + 1 < count) Q[i + 1] = v1 ? (o1.ok ? o1.q : ~0ull) : 0;
+        }
+    }
+}
+
+// ---- statistics: checksum, near count, FLT errors, hits, ordered hash ----
+
+struct FermPart {
+    u64 h, len;          // ordered hash over the segment and its number of terms
+    u64 cks, near, flt, tests;
+};
+
+__device__ __forceinline__ u64 pow_u64(u64 b, u64 e)
+{
+    u64 r = 1;
+    while (e) { if (e & 1) r *= b; b *= b; e >>= 1; }
+    return r;
+}
+
+__device__ __forceinline__ void fp_join(FermPart &L, const FermPart &R)
+{
+    L.h = L.h * pow_u64(MP_FNV_PRIME, R.len) + R.h;
+    L.len += R.len;
+    L.cks += R.cks; L.near += R.near; L.flt += R.flt; L.tests += R.tests;
+}
+
+__global__ void __launch_bounds__(256) fermat_stats_kernel(const u64 *__restrict__ P, const u64 *__restrict__ Q, u64 count,
+                                                            FermPart *parts, u64 *hits, u64 *nhits)
+{
+    __shared__ FermPart s_w[8];
+    const u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    FermPart f = {0, 0, 0, 0, 0, 0};
+    if (i < count) {
+        const u64 p = P[i], q = Q[i];
+        if (p >= 3) {
+            f.tests = 1;
+            if (q >= p) f.flt = 1;
+            else {
+                f.cks = mp_mix64(q ^ (p * MP_GOLD));
+                const u64 A = q <= p / 2 ? q : p - q;
+                f.near = A <= (p - 1) / 1000;              // 1000 A < p
+                f.h = mp_mix64(p ^ mp_mix64(q));
+                f.len = 1;
+                if (q == 0) {
+                    const u64 k = atomicAdd((unsigned long long *)nhits, 1ull);
+                    if (k < 16) hits[k] = p;
+                }
+            }
+        }
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        FermPart r;
+        r.h = __shfl_down_sync(0xffffffffu, f.h, d);
+        r.len = __shfl_down_sync(0xffffffffu, f.len, d);
+        r.cks = __shfl_down_sync(0xffffffffu, f.cks, d);
+        r.near = __shfl_down_sync(0xffffffffu, f.near, d);
+        r.flt = __shfl_down_sync(0xffffffffu, f.flt, d);
+        r.tests = __shfl_down_sync(0xffffffffu, f.tests, d);
+        if ((lane & (2 * d - 1)) == 0 && lane + d < 32) fp_join(f, r);
+    }
+    if (lane == 0) s_w[warp] = f;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        FermPart b = s_w[0];
+        for (int w = 1; w < (int)(blockDim.x >> 5); w++) fp_join(b, s_w[w]);
+        parts[blockIdx.x] = b;
+    }
+}
+
+__global__ void __launch_bounds__(1024) fermat_final_kernel(const FermPart *parts, u64 nparts, const u64 *nhits,
+                                                            const u64 *hits, mp_wief_stats *out)
+{
+    __shared__ FermPart s[1024];
+    const u32 tid = threadIdx.x, nth = blockDim.x;
+    const u64 per = (nparts + nth - 1) / nth;
+    FermPart f = {0, 0, 0, 0, 0, 0};
+    for (u64 b = tid * per; b < (tid + 1) * per && b < nparts; b++) fp_join(f, parts[b]);
+    s[tid] = f;
+    __syncthreads();
+    if (tid == 0) {
+        FermPart g = s[0];
+        for (u32 i = 1; i < nth; i++) fp_join(g, s[i]);
+        out->tests = g.tests;
+        out->near = g.near;
+        out->flt = g.flt;
+        out->cks = g.cks;
+        out->ordered_hash = g.h;
+        out->nhits = *nhits;
+        for (int k = 0; k < 16; k++) out->hits[k] = k < (int)*nhits ? hits[k] : 0;
+    }
+}
+
+// ---- host side ----
+
+int mp_fermat_run(mp_handle *h, const u64 *d_p, u64 count, u64 *d_q, cudaStream_t st, int variant, u64 *)
+{
+    if (!count) return MP_OK;
+    // variant: bit 0 = limbs (0: K=3, 1: K=4); bit 1 = two primes per thread
+    const int k4 = variant & 1, ilp2 = (variant >> 1) & 1;
+    const u64 work = ilp2 ? (count + 1) / 2 : count;
+    u64 grid = (work + 255) / 256;
+    const u64 gmax = (u64)h->sm_count * 64;
+    if (grid > gmax) grid = gmax;
+    ProfScope ps(h, PROF_FERMAT, st);
+    if (!k4 && !ilp2) fermat_kernel<3, 1><<<(unsigned)grid, 256, 0, st>>>(d_p, count, d_q);
+    else if (!k4 && ilp2) fermat_kernel<3, 2><<<(unsigned)grid, 256, 0, st>>>(d_p, count, d_q);
+    else if (k4 && !ilp2) fermat_kernel<4, 1><<<(unsigned)grid, 256, 0, st>>>(d_p, count, d_q);
+    else fermat_kernel<4, 2><<<(unsigned)grid, 256, 0, st>>>(d_p, count, d_q);
+    MP_CUDA(h, cudaGetLastError());
+    return MP_OK;
+}
+
+int mp_fermat_reduce(mp_handle *h, const u64 *d_p, const u64 *d_q, u64 count, mp_wief_stats *d_stats, cudaStream_t st)
+{
+    const u64 nb = count ? (count + 255) / 256 : 1;
+    MP_CUDA(h, h->ferm_part.ensure((size_t)nb * sizeof(FermPart) + 256));
+    FermPart *parts = h->ferm_part.as<FermPart>();
+    u64 *hits = (u64 *)((char *)h->ferm_part.p + nb * sizeof(FermPart));
+    u64 *nhits = hits + 16;
+    MP_CUDA(h, cudaMemsetAsync(hits, 0, 17 * 8, st));
+    if (count) {
+        ProfScope ps(h, PROF_FERMAT_STATS, st);
+        fermat_stats_kernel<<<(unsigned)nb, 256, 0, st>>>(d_p, d_q, count, parts, hits, nhits);
+        MP_CUDA(h, cudaGetLastError());
+    } else {
+        MP_CUDA(h, cudaMemsetAsync(parts, 0, sizeof(FermPart), st));
+    }
+    fermat_final_kernel<<<1, 1024, 0, st>>>(parts, nb, nhits, hits, d_stats);
+    MP_CUDA(h, cudaGetLastError());
+    return MP_OK;
+}

@@ -1,0 +1,1081 @@
+// mp_sieve.cu -- the segmented odd-only sieve of Eratosthenes for B200 (sm_100a) and its
+// scans: prime counts, twin pairs, 6-tuples {0,4,6,10,12,16}, maximal gaps, per-block
+// statistics, per-segment FNV-1a hashes, the prime bitmap and prime lists.
+//
+// Reference behaviour (paths inside the Mathpub project): the odd-only layout and the
+// start of marking at max(q^2, first odd multiple) follow scan_interval in
+// A228768/a228768.c:372-415; small primes applied as periodic patterns follow
+// pattern_setup/presieve in A350826/a350826.c:1192-1271; large primes filed by the segment
+// of their next hit follow the bucket sieve of A007508/a007508.c:282-338,447-480; the gap
+// belongs to the prime that starts it (A000230/a000230.c:12-16); twins and 6-tuples are
+// counted by their first member (A007508/a007508.c:1-10, A350826/a350826.c:22-31) with the
+// tuple checksum sum of mix64(p) (A350826/a350826.c:1364-1379).
+//
+// Layout on the device: bit i of the odd-only map stands for base + 2i + 1 (base = lo & ~1).
+// The map is cut into tiles of 2^TLOG bits (TLOG = 18..20) that live in shared memory, each
+// with a halo of 1024 bits sieved twice so that twins and 6-tuples that start in a tile are
+// decided inside it.  Sieving primes are split into tiers by size:
+//   3..89          five product patterns (periods 4849845, 765049, 4391633, 17120443,
+//                  42600829 bits) ORed into the tile with 128-bit vector loads;
+//   97..2047       one warp per prime, lanes on consecutive multiples, shared atomics;
+//   2048..2^TLOG   one thread per prime, shared atomics;
+//   > 2^TLOG       bucket records: a scatter kernel files the hit offsets of each prime
+//                  for a wave of tiles; the tile kernel ORs them in.
+// A tile summary (count, twins, tuples, checksum, first/last prime, widest internal gap)
+// goes to HBM; a one-CTA fold kernel joins the summaries in order into block and range
+// results, attributing every gap to the prime that starts it.
+#include "mp_common.cuh"
+#include <algorithm>
+#include <math.h>
+#include <stdarg.h>
+
+#define HALO_WORDS 32u
+#define HALO_BITS (HALO_WORDS * 32u)
+#define QWARP 2048u
+#define PAT_MAXQ 89u
+#define MAX_TLOG 20
+
+static const u32 kPatPrimes[MP_NPAT][7] = {
+    {3, 5, 7, 11, 13, 17, 19}, {23, 29, 31, 37, 0}, {41, 43, 47, 53, 0}, {59, 61, 67, 71, 0}, {73, 79, 83, 89, 0}};
+__constant__ u32 c_pat_primes[MP_NPAT][7] = {
+    {3, 5, 7, 11, 13, 17, 19}, {23, 29, 31, 37, 0}, {41, 43, 47, 53, 0}, {59, 61, 67, 71, 0}, {73, 79, 83, 89, 0}};
+
+struct TileSum {
+    u64 first, last;   // first / last prime bit in the tile (bits < nbx); MP_NONE if none
+    u64 lastin;        // last prime bit below limit; MP_NONE if none
+    u64 mgs;           // bit of the prime starting the widest internal gap; MP_NONE if none
+    u64 cks;           // sum of mix64(p) over the 6-tuple starts p (bits < limit)
+    u32 mg;            // widest internal gap in bits (pairs whose first prime is in range)
+    u32 count;         // primes with bit < limit
+    u32 twins, tuples;
+};
+
+struct SieveGeom {
+    u64 base, limit, nbx;   // base even; bits [0, limit) in range; bits [0, nbx) sieved
+    u32 tlog, ntiles;
+};
+
+struct TileArgs {
+    SieveGeom g;
+    u32 t0, nt;                          // tiles [t0, t0 + nt) of this launch
+    const u32 *q;
+    const u64 *magic;
+    u32 iw0, iw1, it1;                   // warp tier [iw0, iw1), thread tier [iw1, it1)
+    const u32 *pat[MP_NPAT];
+    u32 period[MP_NPAT];
+    const u32 *rec;                      // bucket records of tiles [t0, t0 + nt) (nullable)
+    const u32 *reccnt;
+    u32 reccap;
+    TileSum *sums;                       // by global tile index
+    u32 *bitmap32;                       // nullable
+    const u64 *emit_off;                 // emit mode: per-tile offset of its first prime
+    u64 *emit64;
+    u32 *emit32;
+    u32 *queue;
+};
+
+// ---------------------------------------------------------------------------------------
+// ordered combine of tile / thread summaries
+// ---------------------------------------------------------------------------------------
+
+struct Part {
+    u64 first, last, lastin, mgs, cks;
+    u32 mg, count, twins, tuples;
+};
+
+__device__ __forceinline__ void part_init(Part &p)
+{
+    p.first = p.last = p.lastin = p.mgs = MP_NONE;
+    p.cks = 0;
+    p.mg = p.count = p.twins = p.tuples = 0;
+}
+
+// L followed by R (R's bits all above L's); gaps compare strictly so the earliest start wins
+__device__ __forceinline__ Part part_join(const Part &L, const Part &R, u64 limit)
+{
+    Part o;
+    o.count = L.count + R.count;
+    o.twins = L.twins + R.twins;
+    o.tuples = L.tuples + R.tuples;
+    o.cks = L.cks + R.cks;
+    o.mg = L.mg;
+    o.mgs = L.mgs;
+    if (L.first == MP_NONE) {
+        o.first = R.first; o.last = R.last; o.lastin = R.lastin; o.mg = R.mg; o.mgs = R.mgs;
+        return o;
+    }
+    o.first = L.first;
+    if (R.first == MP_NONE) { o.last = L.last; o.lastin = L.lastin; return o; }
+    o.last = R.last;
+    o.lastin = R.lastin != MP_NONE ? R.lastin : L.lastin;
+    if (L.last < limit) {
+        const u32 g = (u32)(R.first - L.last);
+        if (g > o.mg) { o.mg = g; o.mgs = L.last; }
+    }
+    if (R.mg > o.mg) { o.mg = R.mg; o.mgs = R.mgs; }
+    return o;
+}
+
+__device__ __forceinline__ Part part_shfl_down(const Part &p, int d)
+{
+    Part o;
+    o.first = __shfl_down_sync(0xffffffffu, p.first, d);
+    o.last = __shfl_down_sync(0xffffffffu, p.last, d);
+    o.lastin = __shfl_down_sync(0xffffffffu, p.lastin, d);
+    o.mgs = __shfl_down_sync(0xffffffffu, p.mgs, d);
+    o.cks = __shfl_down_sync(0xffffffffu, p.cks, d);
+    o.mg = __shfl_down_sync(0xffffffffu, p.mg, d);
+    o.count = __shfl_down_sync(0xffffffffu, p.count, d);
+    o.twins = __shfl_down_sync(0xffffffffu, p.twins, d);
+    o.tuples = __shfl_down_sync(0xffffffffu, p.tuples, d);
+    return o;
+}
+
+// in-order reduction over the lanes of a warp; lane 0 holds the result
+__device__ __forceinline__ Part part_warp_reduce(Part p, u64 limit)
+{
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        Part r = part_shfl_down(p, d);
+        if ((lane & (2 * d - 1)) == 0) p = part_join(p, r, limit);
+    }
+    return p;
+}
+
+// ---------------------------------------------------------------------------------------
+// tile kernel
+// ---------------------------------------------------------------------------------------
+
+__device__ __forceinline__ u32 bits_mask(u64 start, u64 bound)
+{
+    // bits start .. start+31 below bound
+    if (start >= bound) return 0;
+    const u64 n = bound - start;
+    return n >= 32 ? 0xffffffffu : ((1u << n) - 1);
+}
+
+template <int TLOG>
+__device__ __forceinline__ void presieve(u32 *sm, const TileArgs &a, const u32 *s_off)
+{
+    constexpr u32 NW = (1u << TLOG) / 32 + HALO_WORDS;
+    const u32 tid = threadIdx.x, nth = blockDim.x;
+    for (u32 w4 = tid * 4; w4 < NW; w4 += nth * 4) {
+        u32 o0 = 0, o1 = 0, o2 = 0, o3 = 0;
+#pragma unroll
+        for (int p = 0; p < MP_NPAT; p++) {
+            const u32 bit = s_off[p] + w4 * 32;
+            const u32 s = bit >> 5, sh = bit & 31, a4 = s & ~3u;
+            const uint4 lo = __ldg((const uint4 *)(a.pat[p] + a4));
+            const uint4 hi = __ldg((const uint4 *)(a.pat[p] + a4 + 4));
+            u32 v0, v1, v2, v3, v4;
+            switch (s & 3) {          // uniform across the CTA for a given tile and pattern
+            case 0: v0 = lo.x; v1 = lo.y; v2 = lo.z; v3 = lo.w; v4 = hi.x; break;
+            case 1: v0 = lo.y; v1 = lo.z; v2 = lo.w; v3 = hi.x; v4 = hi.y; break;
+            case 2: v0 = lo.z; v1 = lo.w; v2 = hi.x; v3 = hi.y; v4 = hi.z; break;
+            default: v0 = lo.w; v1 = hi.x; v2 = hi.y; v3 = hi.z; v4 = hi.w; break;
+            }
+            o0 |= __funnelshift_r(v0, v1, sh);
+            o1 |= __funnelshift_r(v1, v2, sh);
+            o2 |= __funnelshift_r(v2, v3, sh);
+            o3 |= __funnelshift_r(v3, v4, sh);
+        }
+        *(uint4 *)&sm[w4] = make_uint4(o0, o1, o2, o3);
+    }
+}
+
+// EMIT = 0: statistics (+ optional bitmap); EMIT = 1: write the in-range primes
+template <int TLOG, int EMIT>
+__global__ void __launch_bounds__(1024) tile_kernel(TileArgs a)
+{
+    constexpr u32 T = 1u << TLOG;
+    constexpr u32 TW = T / 32;
+    constexpr u32 NB = T + HALO_BITS;          // bits held in shared memory
+    extern __shared__ __align__(16) u32 sm[];  // TW + HALO_WORDS words
+    __shared__ u32 s_tile;
+    __shared__ u32 s_off[MP_NPAT];
+    __shared__ Part s_part[32];
+    __shared__ u32 s_cnt[32];
+
+    const u32 tid = threadIdx.x, nth = blockDim.x, lane = tid & 31, warp = tid >> 5, nwarps = nth >> 5;
+    const u64 base = a.g.base, limit = a.g.limit, nbx = a.g.nbx;
+
+    for (;;) {
+        if (tid == 0) s_tile = atomicAdd(a.queue, 1u);
+        __syncthreads();
+        const u32 rel = s_tile;
+        if (rel >= a.nt) break;
+        const u32 t = a.t0 + rel;
+        const u64 G = (u64)t << TLOG;           // first bit of the tile
+        const u64 x0 = base + 2 * G + 1;        // the odd number of that bit
+        if (tid < MP_NPAT) s_off[tid] = (u32)((base / 2 + G) % a.period[tid]);
+        __syncthreads();
+
+        // 1. small primes: patterns
+        presieve<TLOG>(sm, a, s_off);
+        __syncthreads();
+        if (x0 <= PAT_MAXQ && tid == 0) {
+            // the pattern primes themselves are prime; 1 is not
+            for (int p = 0; p < MP_NPAT; p++)
+                for (int k = 0; k < 7 && c_pat_primes[p][k]; k++) {
+                    const u64 q = c_pat_primes[p][k];
+                    if (q >= x0 && ((q - x0) >> 1) < NB) {
+                        const u32 j = (u32)((q - x0) >> 1);
+                        atomicAnd(&sm[j >> 5], ~(1u << (j & 31)));
+                    }
+                }
+            if (x0 == 1) atomicOr(&sm[0], 1u);
+        }
+
+        // 2. warp tier: one warp per prime, lanes on consecutive multiples
+        for (u32 k = a.iw0 + warp; k < a.iw1; k += nwarps) {
+            const u32 q = __ldg(a.q + k);
+            const u32 r = mp_mod_barrett(x0, q, __ldg(a.magic + k));
+            const u32 j0 = (u32)mp_first_odd_multiple(x0, q, r, NB);
+            for (u32 j = j0 + lane * q; j < NB; j += 32 * q) atomicOr(&sm[j >> 5], 1u << (j & 31));
+        }
+        // 3. thread tier: one thread per prime
+        for (u32 k = a.iw1 + tid; k < a.it1; k += nth) {
+            const u32 q = __ldg(a.q + k);
+            const u32 r = mp_mod_barrett(x0, q, __ldg(a.magic + k));
+            for (u32 j = (u32)mp_first_odd_multiple(x0, q, r, NB); j < NB; j += q)
+                atomicOr(&sm[j >> 5], 1u << (j & 31));
+        }
+        // 4. large primes: bucket records of this tile
+        if (a.rec) {
+            u32 n = __ldg(a.reccnt + rel);
+            if (n > a.reccap) n = a.reccap;
+            const u32 *R = a.rec + (u64)rel * a.reccap;
+            for (u32 i = tid; i < n; i += nth) {
+                const u32 j = __ldg(R + i);
+                atomicOr(&sm[j >> 5], 1u << (j & 31));
+            }
+        }
+        __syncthreads();
+
+        // 5. scans: thread `tid` owns words [w0, w1) of the tile
+        const u32 wpt = TW / nth;
+        const u32 w0 = tid * wpt;
+        if (!EMIT) {
+            Part P;
+            part_init(P);
+            for (u32 w = w0; w < w0 + wpt; w++) {
+                const u64 bit0 = G + 32ull * w;
+                const u32 vm = bits_mask(bit0, nbx), lm = bits_mask(bit0, limit);
+                const u32 pw = ~sm[w] & vm;
+                const u32 pn = ~sm[w + 1] & bits_mask(bit0 + 32, nbx);
+                const u32 pin = pw & lm;
+                const u64 x = (u64)pw | ((u64)pn << 32);
+                P.count += __popc(pin);
+                P.twins += __popc(pin & (u32)(x >> 1));
+                u32 tup = pin & (u32)((x >> 2) & (x >> 3) & (x >> 5) & (x >> 6) & (x >> 8));
+                if (tup) {
+                    P.tuples += __popc(tup);
+                    while (tup) {
+                        const u32 b = __ffs(tup) - 1;
+                        tup &= tup - 1;
+                        P.cks += mp_mix64(base + 2 * (bit0 + b) + 1);
+                    }
+                }
+                u32 y = pw;
+                while (y) {
+                    const u32 b = __ffs(y) - 1;
+                    y &= y - 1;
+                    const u64 pos = bit0 + b;
+                    if (P.last == MP_NONE) P.first = pos;
+                    else if (P.last < limit) {
+                        const u32 g = (u32)(pos - P.last);
+                        if (g > P.mg) { P.mg = g; P.mgs = P.last; }
+                    }
+                    P.last = pos;
+                    if (pos < limit) P.lastin = pos;
+                }
+            }
+            P = part_warp_reduce(P, limit);
+            if (lane == 0) s_part[warp] = P;
+            __syncthreads();
+            if (warp == 0) {
+                Part Q;
+                if (lane < nwarps) Q = s_part[lane];
+                else part_init(Q);
+                Q = part_warp_reduce(Q, limit);
+                if (lane == 0) {
+                    TileSum S;
+                    S.first = Q.first; S.last = Q.last; S.lastin = Q.lastin; S.mgs = Q.mgs; S.cks = Q.cks;
+                    S.mg = Q.mg; S.count = Q.count; S.twins = Q.twins; S.tuples = Q.tuples;
+                    a.sums[t] = S;
+                }
+            }
+            if (a.bitmap32) {
+                // in-range prime words, up to the next multiple of 64 bits
+                const u64 lim64 = (limit + 63) & ~63ull;
+                for (u32 w = tid; w < TW; w += nth) {
+                    const u64 bit0 = G + 32ull * w;
+                    if (bit0 >= lim64) break;
+                    a.bitmap32[(G >> 5) + w] = ~sm[w] & bits_mask(bit0, limit);
+                }
+            }
+        } else {
+            // emit: in-range primes in order; per-thread counts, then a CTA-wide scan
+            u32 c = 0;
+            for (u32 w = w0; w < w0 + wpt; w++) c += __popc(~sm[w] & bits_mask(G + 32ull * w, limit));
+            u32 incl = c;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const u32 v = __shfl_up_sync(0xffffffffu, incl, d);
+                if (lane >= (u32)d) incl += v;
+            }
+            if (lane == 31) s_cnt[warp] = incl;
+            __syncthreads();
+            if (warp == 0) {
+                u32 v = lane < nwarps ? s_cnt[lane] : 0, iv = v;
+#pragma unroll
+                for (int d = 1; d < 32; d <<= 1) {
+                    const u32 u = __shfl_up_sync(0xffffffffu, iv, d);
+                    if (lane >= (u32)d) iv += u;
+                }
+                if (lane < nwarps) s_cnt[lane] = iv - v;   // exclusive warp offsets
+            }
+            __syncthreads();
+            u64 pos = a.emit_off[t] + s_cnt[warp] + (incl - c);
+            for (u32 w = w0; w < w0 + wpt; w++) {
+                const u64 bit0 = G + 32ull * w;
+                u32 y = ~sm[w] & bits_mask(bit0, limit);
+                while (y) {
+                    const u32 b = __ffs(y) - 1;
+                    y &= y - 1;
+                    const u64 p = base + 2 * (bit0 + b) + 1;
+                    if (a.emit64) a.emit64[pos] = p;
+                    else a.emit32[pos] = (u32)p;
+                    pos++;
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// bucket scatter for primes > 2^TLOG
+// ---------------------------------------------------------------------------------------
+
+struct ScatterArgs {
+    u64 base;
+    u32 tlog, t0, wt;                // wave = tiles [t0, t0 + wt)
+    u64 nbx;
+    const u32 *q;
+    const u64 *magic;
+    u32 i0, i1;                      // prime index range (large primes)
+    u32 ppb;                         // primes per CTA
+    u32 *rec;                        // [wt][cap]
+    u32 *cnt;                        // [wt], zeroed before the launch
+    u32 cap;
+    u32 *err;
+};
+
+// every hit j of prime q in the wave (plus the first HALO_BITS bits after it): record
+// (tile, offset) for its own tile, and (tile - 1, offset + 2^TLOG) when it lies in the first
+// HALO_BITS bits of a tile, because the previous tile sieves those bits as its halo
+template <int PASS>
+__device__ __forceinline__ void scatter_prime(const ScatterArgs &a, u32 k, u64 x0, u64 wstart, u64 wend_halo,
+                                              u32 *scnt, const u32 *sbase)
+{
+    const u32 q = __ldg(a.q + k);
+    const u32 r = mp_mod_barrett(x0, q, __ldg(a.magic + k));
+    u64 j = wstart + mp_first_odd_multiple(x0, q, r, wend_halo - wstart);
+    const u32 T = 1u << a.tlog;
+    for (; j < wend_halo; j += q) {
+        const u32 tl = (u32)(j >> a.tlog) - a.t0;    // tile relative to the wave
+        const u32 off = (u32)j & (T - 1);
+        if (tl < a.wt) {
+            if (PASS == 0) atomicAdd(&scnt[tl], 1u);
+            else {
+                const u32 slot = sbase[tl] + atomicAdd(&scnt[tl], 1u);
+                if (slot < a.cap) a.rec[(u64)tl * a.cap + slot] = off;
+                else atomicOr(a.err, 2u);
+            }
+        }
+        if (off < HALO_BITS && tl >= 1 && tl - 1 < a.wt) {
+            if (PASS == 0) atomicAdd(&scnt[tl - 1], 1u);
+            else {
+                const u32 slot = sbase[tl - 1] + atomicAdd(&scnt[tl - 1], 1u);
+                if (slot < a.cap) a.rec[(u64)(tl - 1) * a.cap + slot] = off + T;
+                else atomicOr(a.err, 2u);
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(512) scatter_kernel(ScatterArgs a)
+{
+    extern __shared__ u32 ssm[];             // scnt[wt], sbase[wt]
+    u32 *scnt = ssm, *sbase = ssm + a.wt;
+    const u32 tid = threadIdx.x, nth = blockDim.x;
+    for (u32 i = tid; i < a.wt; i += nth) scnt[i] = 0;
+    __syncthreads();
+    const u64 wstart = (u64)a.t0 << a.tlog;
+    u64 wend = (u64)(a.t0 + a.wt) << a.tlog;
+    if (wend > a.nbx) wend = a.nbx;
+    u64 wend_halo = wend + HALO_BITS;
+    if (wend_halo > a.nbx) wend_halo = a.nbx;
+    const u64 x0 = a.base + 2 * wstart + 1;
+    const u32 k0 = a.i0 + blockIdx.x * a.ppb;
+    u32 k1 = k0 + a.ppb;
+    if (k1 > a.i1) k1 = a.i1;
+    for (u32 k = k0 + tid; k < k1; k += nth) scatter_prime<0>(a, k, x0, wstart, wend_halo, scnt, sbase);
+    __syncthreads();
+    for (u32 i = tid; i < a.wt; i += nth) {
+        const u32 c = scnt[i];
+        sbase[i] = c ? atomicAdd(a.cnt + i, c) : 0;
+        scnt[i] = 0;
+    }
+    __syncthreads();
+    for (u32 k = k0 + tid; k < k1; k += nth) scatter_prime<1>(a, k, x0, wstart, wend_halo, scnt, sbase);
+}
+
+// ---------------------------------------------------------------------------------------
+// fold: tile summaries -> block and range results
+// ---------------------------------------------------------------------------------------
+
+struct FoldArgs {
+    u64 base, limit, lo, hi;
+    const TileSum *sums;
+    u32 ntiles, tpb;                 // tiles per block
+    u32 nblocks, nblocks_ext;        // blocks in range / over all tiles
+    Part *acc;                       // scratch [nblocks_ext]
+    mp_range_stats *out;
+    mp_block_stats *blocks;          // nullable
+    u32 *err;
+    int has2;
+};
+
+__device__ __forceinline__ Part tile_part(const TileSum &S)
+{
+    Part p;
+    p.first = S.first; p.last = S.last; p.lastin = S.lastin; p.mgs = S.mgs; p.cks = S.cks;
+    p.mg = S.mg; p.count = S.count; p.twins = S.twins; p.tuples = S.tuples;
+    return p;
+}
+
+__device__ __forceinline__ void stats_from_part(mp_range_stats &o, const Part &p, u64 base, u64 limit, u64 nprimes_u64)
+{
+    o.pi = nprimes_u64;
+    o.twins = p.twins;
+    o.tuple6 = p.tuples;
+    o.tuple6_cks = p.cks;
+    o.max_gap = p.mgs == MP_NONE ? 0 : 2ull * p.mg;
+    o.gap_start = p.mgs == MP_NONE ? 0 : base + 2 * p.mgs + 1;
+    o.first_prime = (p.first == MP_NONE || p.first >= limit) ? 0 : base + 2 * p.first + 1;
+    o.last_prime = p.lastin == MP_NONE ? 0 : base + 2 * p.lastin + 1;
+}
+
+struct RangeAcc {
+    u64 n, tw, tu, cks, first, lastin, mgs;
+    u32 mg;
+};
+
+__device__ __forceinline__ void racc_init(RangeAcc &r)
+{
+    r.n = r.tw = r.tu = r.cks = 0;
+    r.first = r.lastin = r.mgs = MP_NONE;
+    r.mg = 0;
+}
+
+// append block part B (bits above everything in r)
+__device__ __forceinline__ void racc_add(RangeAcc &r, const Part &B)
+{
+    r.n += B.count; r.tw += B.twins; r.tu += B.tuples; r.cks += B.cks;
+    if (r.first == MP_NONE) r.first = B.first;
+    if (B.lastin != MP_NONE) r.lastin = B.lastin;
+    if (B.mgs != MP_NONE && (r.mgs == MP_NONE || B.mg > r.mg)) { r.mg = B.mg; r.mgs = B.mgs; }
+}
+
+__device__ __forceinline__ void racc_join(RangeAcc &r, const RangeAcc &B)
+{
+    r.n += B.n; r.tw += B.tw; r.tu += B.tu; r.cks += B.cks;
+    if (r.first == MP_NONE) r.first = B.first;
+    if (B.lastin != MP_NONE) r.lastin = B.lastin;
+    if (B.mgs != MP_NONE && (r.mgs == MP_NONE || B.mg > r.mg)) { r.mg = B.mg; r.mgs = B.mgs; }
+}
+
+// 64-bit totals: block parts carry u32 counts (a block is at most 2^31 bits); the range
+// total is summed in 64 bits
+__global__ void __launch_bounds__(512) fold_kernel(FoldArgs a)
+{
+    const u32 tid = threadIdx.x, nth = blockDim.x;
+    // 1. blocks (over all tiles, including the tail)
+    for (u32 b = tid; b < a.nblocks_ext; b += nth) {
+        Part P;
+        part_init(P);
+        const u32 t0 = b * a.tpb;
+        u32 t1 = t0 + a.tpb;
+        if (t1 > a.ntiles) t1 = a.ntiles;
+        for (u32 t = t0; t < t1; t++) P = part_join(P, tile_part(a.sums[t]), a.limit);
+        a.acc[b] = P;
+    }
+    __syncthreads();
+    // 2. trailing gap of each in-range block: from its last prime to the first prime of a
+    //    later block
+    for (u32 b = tid; b < a.nblocks; b += nth) {
+        Part P = a.acc[b];
+        if (P.last != MP_NONE && P.last < a.limit) {
+            u64 nf = MP_NONE;
+            for (u32 c = b + 1; c < a.nblocks_ext; c++) {
+                const u64 f = a.acc[c].first;
+                if (f != MP_NONE) { nf = f; break; }
+            }
+            if (nf == MP_NONE) atomicOr(a.err, 4u);
+            else {
+                const u32 g = (u32)(nf - P.last);
+                if (g > P.mg) { a.acc[b].mg = g; a.acc[b].mgs = P.last; }
+            }
+        }
+    }
+    __syncthreads();
+    // 3. block outputs (prime 2 joins the block that holds it)
+    if (a.blocks) {
+        for (u32 b = tid; b < a.nblocks; b += nth) {
+            const Part P = a.acc[b];
+            mp_range_stats o;
+            stats_from_part(o, P, a.base, a.limit, P.count);
+            if (a.has2 && b == 0) {
+                o.pi += 1;
+                o.first_prime = 2;
+                if (P.lastin == MP_NONE) o.last_prime = 2;
+                if (o.max_gap <= 1) { o.max_gap = 1; o.gap_start = 2; }
+            }
+            a.blocks[b] = o;
+        }
+    }
+    // 4. range: in-order join of the in-range blocks, whose parts already hold their
+    //    trailing gaps (each thread a contiguous run of blocks, then thread 0 in order)
+    __shared__ RangeAcc s_r[512];
+    {
+        const u32 per = (a.nblocks + nth - 1) / nth;
+        RangeAcc R;
+        racc_init(R);
+        for (u32 b = tid * per; b < (tid + 1) * per && b < a.nblocks; b++) racc_add(R, a.acc[b]);
+        s_r[tid] = R;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        RangeAcc R;
+        racc_init(R);
+        for (u32 i = 0; i < nth; i++) racc_join(R, s_r[i]);
+        mp_range_stats o;
+        o.pi = R.n;
+        o.twins = R.tw;
+        o.tuple6 = R.tu;
+        o.tuple6_cks = R.cks;
+        o.max_gap = R.mgs == MP_NONE ? 0 : 2ull * R.mg;
+        o.gap_start = R.mgs == MP_NONE ? 0 : a.base + 2 * R.mgs + 1;
+        o.first_prime = (R.first == MP_NONE || R.first >= a.limit) ? 0 : a.base + 2 * R.first + 1;
+        o.last_prime = R.lastin == MP_NONE ? 0 : a.base + 2 * R.lastin + 1;
+        if (a.has2) {
+            o.pi += 1;
+            o.first_prime = 2;
+            if (R.lastin == MP_NONE) o.last_prime = 2;
+            if (o.max_gap <= 1) { o.max_gap = 1; o.gap_start = 2; }
+        }
+        *a.out = o;
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// FNV-1a-64 per hash segment of the bitmap (one thread per segment: the hash is a chain)
+// ---------------------------------------------------------------------------------------
+
+__global__ void hash_kernel(const u32 *__restrict__ bm, u64 nbits, u64 seg_bits, u64 nseg, u64 *out)
+{
+    const u64 s = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nseg) return;
+    const u64 b0 = s * seg_bits;
+    const u64 len = b0 + seg_bits <= nbits ? seg_bits : nbits - b0;
+    const u64 nbytes = (len + 7) >> 3;
+    const u8 *p = (const u8 *)bm + (b0 >> 3);       // seg_bits is a multiple of 8
+    u64 h = MP_FNV_OFFSET;
+    u64 k = 0;
+    // 16-byte loads where aligned
+    while (k < nbytes && (((uintptr_t)(p + k)) & 15)) { h ^= p[k]; h *= MP_FNV_PRIME; k++; }
+    for (; k + 16 <= nbytes; k += 16) {
+        const uint4 v = __ldg((const uint4 *)(p + k));
+        const u32 w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+#pragma unroll
+            for (int j = 0; j < 4; j++) { h ^= (w[i] >> (8 * j)) & 0xff; h *= MP_FNV_PRIME; }
+    }
+    for (; k < nbytes; k++) {
+        u8 c = p[k];
+        const u64 rem = len - 8 * k;
+        if (rem < 8) c &= (u8)((1u << rem) - 1);
+        h ^= c; h *= MP_FNV_PRIME;
+    }
+    out[s] = h;
+}
+
+// exclusive prefix of tile counts -> emit offsets; total to *total (one CTA)
+__global__ void __launch_bounds__(1024) tile_scan_kernel(const TileSum *sums, u32 ntiles, u64 *off, u64 *total)
+{
+    __shared__ u64 s[1024];
+    const u32 tid = threadIdx.x, nth = blockDim.x;
+    const u32 per = (ntiles + nth - 1) / nth;
+    u64 c = 0;
+    for (u32 t = tid * per; t < (tid + 1) * per && t < ntiles; t++) c += sums[t].count;
+    s[tid] = c;
+    __syncthreads();
+    if (tid == 0) {
+        u64 acc = 0;
+        for (u32 i = 0; i < nth; i++) { const u64 v = s[i]; s[i] = acc; acc += v; }
+        *total = acc;
+    }
+    __syncthreads();
+    u64 acc = s[tid];
+    for (u32 t = tid * per; t < (tid + 1) * per && t < ntiles; t++) { off[t] = acc; acc += sums[t].count; }
+}
+
+// ---------------------------------------------------------------------------------------
+// tables: bootstrap primes, big table, Barrett constants, patterns
+// ---------------------------------------------------------------------------------------
+
+// odd primes below 2^16, in one CTA: sieve of Eratosthenes over the odd numbers, then an
+// ordered compaction
+__global__ void __launch_bounds__(1024) boot_primes_kernel(u32 *out, u32 *count)
+{
+    __shared__ u8 comp[32768];      // odd j: 2j + 1 < 65536
+    __shared__ u32 s_cnt[1024];
+    const u32 tid = threadIdx.x, nth = blockDim.x;
+    for (u32 j = tid; j < 32768; j += nth) comp[j] = 0;
+    __syncthreads();
+    comp[0] = 1;   // 1
+    for (u32 q = 3; q * q < 65536; q += 2) {
+        __syncthreads();
+        if (comp[q >> 1]) continue;             // uniform: every thread reads the same byte
+        for (u32 m = q * q + 2 * q * tid; m < 65536; m += 2 * q * nth) comp[m >> 1] = 1;
+    }
+    __syncthreads();
+    const u32 per = 32768 / nth;
+    u32 c = 0;
+    for (u32 j = tid * per; j < (tid + 1) * per; j++) c += !comp[j];
+    s_cnt[tid] = c;
+    __syncthreads();
+    if (tid == 0) {
+        u32 acc = 0;
+        for (u32 i = 0; i < nth; i++) { const u32 v = s_cnt[i]; s_cnt[i] = acc; acc += v; }
+        *count = acc;
+    }
+    __syncthreads();
+    u32 pos = s_cnt[tid];
+    for (u32 j = tid * per; j < (tid + 1) * per; j++)
+        if (!comp[j]) out[pos++] = 2 * j + 1;
+}
+
+__global__ void magic_kernel(const u32 *q, u64 n, u64 *magic)
+{
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x)
+        magic[i] = ~0ull / q[i];
+}
+
+// pattern p: bit j set iff 2j + 1 is divisible by one of the pattern's primes
+__global__ void pattern_kernel(u32 *w, u64 nwords, u32 q0, u32 q1, u32 q2, u32 q3, u32 q4, u32 q5, u32 q6)
+{
+    const u32 qs[7] = {q0, q1, q2, q3, q4, q5, q6};
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < nwords; i += (u64)gridDim.x * blockDim.x) {
+        u32 v = 0;
+        for (u32 b = 0; b < 32; b++) {
+            const u64 x = 2 * (32 * i + b) + 1;
+            for (int k = 0; k < 7; k++)
+                if (qs[k] && x % qs[k] == 0) { v |= 1u << b; break; }
+        }
+        w[i] = v;
+    }
+}
+
+u64 PrimeTable::count_le(u64 x) const
+{
+    return (u64)(std::upper_bound(host.begin(), host.end(), (u32)(x > 0xffffffffull ? 0xffffffffull : x)) - host.begin());
+}
+
+int mp_patterns_ensure(mp_handle *h)
+{
+    if (h->pat_ready) return MP_OK;
+    const u64 slack_bits = (1ull << MAX_TLOG) + HALO_BITS + 8 * 32 + 256;
+    for (int p = 0; p < MP_NPAT; p++) {
+        u64 per = 1;
+        for (int k = 0; k < 7 && kPatPrimes[p][k]; k++) per *= kPatPrimes[p][k];
+        h->pat.period[p] = (u32)per;
+        const u64 words = (per + slack_bits) / 32 + 16;
+        h->pat.words[p] = words;
+        MP_CUDA(h, cudaMalloc(&h->pat.d_words[p], words * 4));
+        const u32 *Q = kPatPrimes[p];
+        pattern_kernel<<<1024, 256, 0, h->stream>>>(h->pat.d_words[p], words, Q[0], Q[1], Q[2], Q[3], Q[4], Q[5], Q[6]);
+        MP_CUDA(h, cudaGetLastError());
+    }
+    MP_CUDA(h, cudaStreamSynchronize(h->stream));
+    h->pat_ready = true;
+    return MP_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+// host driver
+// ---------------------------------------------------------------------------------------
+
+struct Tiers { u32 iw0, iw1, it1, iend; };
+
+static Tiers tiers_for(const PrimeTable &tb, u32 tlog, u64 top)
+{
+    Tiers r;
+    const u64 sq = mp_isqrt64(top - 1) + 1;
+    r.iend = (u32)tb.count_le(sq);
+    r.iw0 = (u32)std::min<u64>(tb.count_le(PAT_MAXQ), r.iend);
+    r.iw1 = (u32)std::min<u64>(tb.count_le(QWARP - 1), r.iend);
+    r.it1 = (u32)std::min<u64>(tb.count_le(1ull << tlog), r.iend);
+    return r;
+}
+
+template <int TLOG, int EMIT>
+static cudaError_t launch_tile(const TileArgs &a, int grid, int nth, cudaStream_t st)
+{
+    const size_t smem = ((1u << TLOG) / 32 + HALO_WORDS) * 4;
+    static bool attr_set[16][64] = {{false}};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const int key = TLOG * 2 + EMIT;
+    if (dev < 0 || dev >= 16) return cudaErrorInvalidDevice;
+    if (!attr_set[dev][key]) {
+        cudaError_t e = cudaFuncSetAttribute(tile_kernel<TLOG, EMIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        attr_set[dev][key] = true;
+    }
+    tile_kernel<TLOG, EMIT><<<grid, nth, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+static cudaError_t launch_tile_any(const TileArgs &a, int grid, int nth, int emit, cudaStream_t st)
+{
+    switch (a.g.tlog * 2 + emit) {
+    case 36: return launch_tile<18, 0>(a, grid, nth, st);
+    case 37: return launch_tile<18, 1>(a, grid, nth, st);
+    case 38: return launch_tile<19, 0>(a, grid, nth, st);
+    case 39: return launch_tile<19, 1>(a, grid, nth, st);
+    case 40: return launch_tile<20, 0>(a, grid, nth, st);
+    case 41: return launch_tile<20, 1>(a, grid, nth, st);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+// resident CTAs per SM for the tile kernel at this geometry
+static int tile_ctas_per_sm(u32 tlog, int nth)
+{
+    const size_t smem = ((1u << tlog) / 32 + HALO_WORDS) * 4 + 2048;
+    int by_smem = (int)((227 * 1024) / smem);
+    int by_thr = 2048 / nth;
+    int r = std::min(by_smem, by_thr);
+    return r < 1 ? 1 : r;
+}
+
+// expected bucket records per tile for the large primes (Mertens' theorem: the sum of 1/q
+// over primes in (a, b] is about ln(ln b / ln a)), with a margin
+static u32 bucket_cap(u32 tlog, u64 qmax)
+{
+    const double T = (double)(1u << tlog) + HALO_BITS;
+    const double a = (double)(1u << tlog);
+    double s = qmax > (u64)a ? log(log((double)qmax) / log(a)) : 0.0;
+    double e = T * s * 1.06 + 8.0 * sqrt(T * s + 1.0) + 4096.0;
+    if (e > 4.0e9) e = 4.0e9;
+    return (u32)e;
+}
+
+struct SievePlan {
+    SieveGeom g;
+    Tiers ti;
+    int nth;
+    bool large;
+    u32 wt, cap, nwaves;
+};
+
+static int plan_sieve(mp_handle *h, const PrimeTable &tb, u64 lo, u64 hi, u32 tlog, int nth, SievePlan &P)
+{
+    P.g.base = lo & ~1ull;
+    P.g.limit = (hi - P.g.base) >> 1;
+    const u64 top = hi + MP_TAIL;
+    P.g.nbx = (top - P.g.base) >> 1;
+    P.g.tlog = tlog;
+    const u64 ntiles = (P.g.nbx + (1ull << tlog) - 1) >> tlog;
+    if (ntiles >= (1ull << 31)) return mp_set_error(h, MP_ERANGE, "range too long (%llu tiles)", (unsigned long long)ntiles);
+    P.g.ntiles = (u32)ntiles;
+    P.ti = tiers_for(tb, tlog, top);
+    if (tb.limit < mp_isqrt64(top - 1)) return mp_set_error(h, MP_EINVAL, "prime table too small");
+    P.nth = nth;
+    P.large = P.ti.iend > P.ti.it1;
+    if (P.large) {
+        const u64 qmax = tb.host[P.ti.iend - 1];
+        P.cap = bucket_cap(tlog, qmax);
+        // wave: at most 64 MB of records per wave and at most 256 tiles
+        u64 wt = (64ull << 20) / ((u64)P.cap * 4);
+        if (wt < 1) wt = 1;
+        if (wt > 256) wt = 256;
+        if (wt > P.g.ntiles) wt = P.g.ntiles;
+        P.wt = (u32)wt;
+        P.nwaves = (P.g.ntiles + P.wt - 1) / P.wt;
+    } else {
+        P.cap = 0; P.wt = P.g.ntiles; P.nwaves = 1;
+    }
+    return MP_OK;
+}
+
+static void fill_tile_args(mp_handle *h, const PrimeTable &tb, const SievePlan &P, TileArgs &a)
+{
+    memset(&a, 0, sizeof a);
+    a.g = P.g;
+    a.q = tb.q.as<u32>();
+    a.magic = tb.magic.as<u64>();
+    a.iw0 = P.ti.iw0; a.iw1 = P.ti.iw1; a.it1 = P.ti.it1;
+    for (int p = 0; p < MP_NPAT; p++) { a.pat[p] = h->pat.d_words[p]; a.period[p] = h->pat.period[p]; }
+}
+
+// mode: 0 batched (waves of persistent tile launches), 1 plain (one launch per tile)
+static int run_tiles(mp_handle *h, const PrimeTable &tb, const SievePlan &P, TileArgs a, int mode, int emit,
+                     cudaStream_t st)
+{
+    const int nth = P.nth;
+    const u32 nlaunch = mode == 1 ? P.g.ntiles : P.nwaves;
+    MP_CUDA(h, h->queue.ensure((size_t)nlaunch * 4 + 64));
+    MP_CUDA(h, cudaMemsetAsync(h->queue.p, 0, (size_t)nlaunch * 4 + 64, st));
+    u32 *errp = h->errflag.as<u32>();
+    if (P.large) {
+        const u32 wt = mode == 1 ? 1 : P.wt;
+        MP_CUDA(h, h->rec.ensure((size_t)wt * P.cap * 4));
+        MP_CUDA(h, h->reccnt.ensure((size_t)wt * 4 * 2));
+    }
+    const int grid_pers = h->sm_count * tile_ctas_per_sm(P.g.tlog, nth);
+    for (u32 L = 0; L < nlaunch; L++) {
+        const u32 t0 = mode == 1 ? L : L * P.wt;
+        const u32 nt = mode == 1 ? 1 : std::min(P.wt, P.g.ntiles - t0);
+        if (P.large) {
+            ScatterArgs s;
+            s.base = P.g.base; s.tlog = P.g.tlog; s.t0 = t0; s.wt = nt; s.nbx = P.g.nbx;
+            s.q = tb.q.as<u32>(); s.magic = tb.magic.as<u64>();
+            s.i0 = P.ti.it1; s.i1 = P.ti.iend;
+            s.ppb = 2048;
+            s.rec = h->rec.as<u32>(); s.cnt = h->reccnt.as<u32>(); s.cap = P.cap; s.err = errp;
+            MP_CUDA(h, cudaMemsetAsync(s.cnt, 0, (size_t)nt * 4, st));
+            const u32 nblk = (P.ti.iend - P.ti.it1 + s.ppb - 1) / s.ppb;
+            {
+                ProfScope ps(h, PROF_SCATTER, st);
+                scatter_kernel<<<nblk, 512, (size_t)nt * 8, st>>>(s);
+            }
+            MP_CUDA(h, cudaGetLastError());
+            a.rec = s.rec; a.reccnt = s.cnt; a.reccap = P.cap;
+        }
+        a.t0 = t0; a.nt = nt;
+        a.queue = h->queue.as<u32>() + L;
+        const int grid = mode == 1 ? 1 : (int)std::min<u64>((u64)grid_pers, nt);
+        ProfScope ps(h, PROF_TILE, st);
+        MP_CUDA(h, launch_tile_any(a, grid, nth, emit, st));
+    }
+    return MP_OK;
+}
+
+static int check_errflag(mp_handle *h, cudaStream_t st)
+{
+    MP_CUDA(h, cudaMemcpyAsync(h->h_err, h->errflag.p, 4, cudaMemcpyDeviceToHost, st));
+    MP_CUDA(h, cudaStreamSynchronize(st));
+    const u32 e = *h->h_err;
+    if (e) {
+        MP_CUDA(h, cudaMemsetAsync(h->errflag.p, 0, 4, st));
+        if (e & 2) return mp_set_error(h, MP_EOVERFLOW, "bucket records exceeded their capacity");
+        if (e & 4) return mp_set_error(h, MP_ERANGE, "no prime follows the last prime of the range within the tail");
+        return mp_set_error(h, MP_ETIMEOUT, "device error flag 0x%x", e);
+    }
+    return MP_OK;
+}
+
+int mp_tables_ensure(mp_handle *h, u64 limit)
+{
+    MP_TRY(mp_patterns_ensure(h));
+    cudaStream_t st = h->stream;
+    if (!h->boot.n) {
+        MP_CUDA(h, h->boot.q.ensure(6600 * 4));
+        MP_CUDA(h, h->boot.magic.ensure(6600 * 8));
+        MP_CUDA(h, h->small_out.ensure(64));
+        boot_primes_kernel<<<1, 1024, 0, st>>>(h->boot.q.as<u32>(), h->small_out.as<u32>());
+        MP_CUDA(h, cudaGetLastError());
+        u32 n = 0;
+        MP_CUDA(h, cudaMemcpyAsync(&n, h->small_out.p, 4, cudaMemcpyDeviceToHost, st));
+        MP_CUDA(h, cudaStreamSynchronize(st));
+        h->boot.n = n;
+        h->boot.limit = 65536;   // every prime <= 65536 (65536 itself is not prime)
+        magic_kernel<<<64, 256, 0, st>>>(h->boot.q.as<u32>(), n, h->boot.magic.as<u64>());
+        MP_CUDA(h, cudaGetLastError());
+        h->boot.host.resize(n);
+        MP_CUDA(h, cudaMemcpyAsync(h->boot.host.data(), h->boot.q.p, (size_t)n * 4, cudaMemcpyDeviceToHost, st));
+        MP_CUDA(h, cudaStreamSynchronize(st));
+    }
+    if (limit <= h->table.limit) return MP_OK;
+    u64 L = std::max<u64>(limit, std::max<u64>(1ull << 22, 2 * h->table.limit));
+    if (L > 0xffffffffull) L = 0xffffffffull;
+    if (limit > L) return mp_set_error(h, MP_ERANGE, "sieving primes above 2^32 are not supported");
+    // sieve [3, L] with the bootstrap primes and emit the odd primes as u32
+    SievePlan P;
+    const u64 lo = 3, hi = L + 1;
+    MP_TRY(plan_sieve(h, h->boot, lo, hi, 20, 1024, P));
+    // the tail is not needed for a prime list, but plan_sieve adds it; primes beyond hi are
+    // not emitted (limit bits)
+    MP_CUDA(h, h->tilesum.ensure((size_t)P.g.ntiles * sizeof(TileSum)));
+    MP_CUDA(h, h->blockacc.ensure((size_t)P.g.ntiles * 8 + 16));
+    TileArgs a;
+    fill_tile_args(h, h->boot, P, a);
+    a.sums = h->tilesum.as<TileSum>();
+    MP_TRY(run_tiles(h, h->boot, P, a, 0, 0, st));
+    u64 *off = h->blockacc.as<u64>();
+    tile_scan_kernel<<<1, 1024, 0, st>>>(a.sums, P.g.ntiles, off, off + P.g.ntiles);
+    MP_CUDA(h, cudaGetLastError());
+    u64 total = 0;
+    MP_CUDA(h, cudaMemcpyAsync(&total, off + P.g.ntiles, 8, cudaMemcpyDeviceToHost, st));
+    MP_CUDA(h, cudaStreamSynchronize(st));
+    h->table.q.release();
+    h->table.magic.release();
+    h->table.n = 0;
+    h->table.limit = 0;
+    MP_CUDA(h, h->table.q.ensure((size_t)total * 4 + 64));
+    MP_CUDA(h, h->table.magic.ensure((size_t)total * 8 + 64));
+    a.emit_off = off;
+    a.emit32 = h->table.q.as<u32>();
+    a.emit64 = nullptr;
+    MP_TRY(run_tiles(h, h->boot, P, a, 0, 1, st));
+    magic_kernel<<<1024, 256, 0, st>>>(h->table.q.as<u32>(), total, h->table.magic.as<u64>());
+    MP_CUDA(h, cudaGetLastError());
+    h->table.host.resize(total);
+    MP_CUDA(h, cudaMemcpyAsync(h->table.host.data(), h->table.q.p, (size_t)total * 4, cudaMemcpyDeviceToHost, st));
+    MP_CUDA(h, cudaStreamSynchronize(st));
+    MP_TRY(check_errflag(h, st));
+    h->table.n = total;
+    h->table.limit = L;
+    return MP_OK;
+}
+
+static int pick_geometry(mp_handle *h, const mp_sieve_opts *o, u32 &tlog, int &nth)
+{
+    tlog = o && o->tile_log2 ? o->tile_log2 : (h->tune.sieve_tile_log2 ? (u32)h->tune.sieve_tile_log2 : 20);
+    nth = o && o->threads ? (int)o->threads : (h->tune.sieve_threads ? h->tune.sieve_threads : 1024);
+    if (tlog < 18 || tlog > 20) return mp_set_error(h, MP_EINVAL, "tile_log2 must be 18, 19 or 20");
+    if (nth != 256 && nth != 512 && nth != 1024) return mp_set_error(h, MP_EINVAL, "threads must be 256, 512 or 1024");
+    return MP_OK;
+}
+
+int mp_sieve_run(mp_handle *h, u64 lo, u64 hi, const mp_sieve_opts *o, mp_range_stats *d_out,
+                 mp_block_stats *d_blocks, u64 *d_hash, u64 *d_bitmap, cudaStream_t st)
+{
+    if (hi <= lo) return mp_set_error(h, MP_EINVAL, "need lo < hi");
+    if (hi > MP_HI_MAX) return mp_set_error(h, MP_ERANGE, "hi must be <= 2^64 - 2^18");
+    if (!d_out) return mp_set_error(h, MP_EINVAL, "null output");
+    const u32 mode = o ? o->mode : MP_MODE_BATCHED;
+    if (mode > 1) return mp_set_error(h, MP_EINVAL, "bad mode");
+    u32 tlog;
+    int nth;
+    MP_TRY(pick_geometry(h, o, tlog, nth));
+    if (mode == MP_MODE_PLAIN && !(o && o->tile_log2)) tlog = 18;   // the reference's 32 KiB segment
+    const u32 block_log2 = o ? o->block_log2 : 0, hash_log2 = o ? o->hash_log2 : 0;
+    if (block_log2 && (block_log2 < tlog + 1 || block_log2 > 32))
+        return mp_set_error(h, MP_EINVAL, "block_log2 must be 0 or in [tile_log2 + 1, 32]");
+    if (hash_log2 && (hash_log2 < 4 || hash_log2 > 40)) return mp_set_error(h, MP_EINVAL, "hash_log2 must be 0 or 4..40");
+    if (d_blocks && !block_log2) return mp_set_error(h, MP_EINVAL, "blocks requested without block_log2");
+    const u64 top = hi + MP_TAIL;
+    MP_TRY(mp_tables_ensure(h, mp_isqrt64(top - 1)));
+    SievePlan P;
+    MP_TRY(plan_sieve(h, h->table, lo, hi, tlog, nth, P));
+    MP_CUDA(h, h->tilesum.ensure((size_t)P.g.ntiles * sizeof(TileSum)));
+    // bitmap: the caller's, or scratch when only hashes are wanted
+    const u64 nwords64 = (P.g.limit + 63) >> 6;
+    u32 *bm = (u32 *)d_bitmap;
+    if (!bm && hash_log2) {
+        MP_CUDA(h, h->scratch_bitmap.ensure((size_t)nwords64 * 8 + 64));
+        bm = h->scratch_bitmap.as<u32>();
+    }
+    TileArgs a;
+    fill_tile_args(h, h->table, P, a);
+    a.sums = h->tilesum.as<TileSum>();
+    a.bitmap32 = bm;
+    MP_TRY(run_tiles(h, h->table, P, a, (int)mode, 0, st));
+    // fold
+    u32 tpb;
+    u64 nblocks;
+    if (block_log2) {
+        tpb = 1u << (block_log2 - 1 - tlog);
+        nblocks = ((hi - lo - 1) >> block_log2) + 1;
+    } else {
+        tpb = 8;
+        while ((P.g.ntiles + tpb - 1) / tpb > 65536) tpb *= 2;
+        const u64 bb = (u64)tpb << tlog;
+        nblocks = (P.g.limit + bb - 1) / bb;
+        if (nblocks == 0) nblocks = 1;
+    }
+    const u64 nbe = (P.g.ntiles + tpb - 1) / tpb;
+    if (nbe > (1ull << 26)) return mp_set_error(h, MP_ERANGE, "too many blocks");
+    MP_CUDA(h, h->blockacc.ensure((size_t)nbe * sizeof(Part)));
+    FoldArgs f;
+    f.base = P.g.base; f.limit = P.g.limit; f.lo = lo; f.hi = hi;
+    f.sums = a.sums; f.ntiles = P.g.ntiles; f.tpb = tpb;
+    f.nblocks = (u32)std::min<u64>(nblocks, nbe); f.nblocks_ext = (u32)nbe;
+    f.acc = h->blockacc.as<Part>();
+    f.out = d_out; f.blocks = d_blocks; f.err = h->errflag.as<u32>();
+    f.has2 = lo <= 2 && 2 < hi;
+    {
+        ProfScope ps(h, PROF_FOLD, st);
+        fold_kernel<<<1, 512, 0, st>>>(f);
+    }
+    MP_CUDA(h, cudaGetLastError());
+    if (hash_log2) {
+        const u64 sb = 1ull << (hash_log2 - 1);
+        const u64 ns = (P.g.limit + sb - 1) / sb;
+        ProfScope ps(h, PROF_HASH, st);
+        hash_kernel<<<(unsigned)((ns + 127) / 128), 128, 0, st>>>(bm, P.g.limit, sb, ns, d_hash);
+        MP_CUDA(h, cudaGetLastError());
+    }
+    return MP_OK;
+}
+
+int mp_sieve_errors(mp_handle *h, cudaStream_t st) { return check_errflag(h, st); }
+
+// all primes in [lo, hi) to d_primes (cap entries); *count = number of primes; synchronises
+int mp_sieve_emit_primes(mp_handle *h, u64 lo, u64 hi, u64 *d_primes, u64 cap, u64 *count, cudaStream_t st)
+{
+    if (hi <= lo) { *count = 0; return MP_OK; }
+    if (hi > MP_HI_MAX) return mp_set_error(h, MP_ERANGE, "hi must be <= 2^64 - 2^18");
+    u32 tlog;
+    int nth;
+    MP_TRY(pick_geometry(h, nullptr, tlog, nth));
+    const u64 top = hi + MP_TAIL;
+    MP_TRY(mp_tables_ensure(h, mp_isqrt64(top - 1)));
+    SievePlan P;
+    MP_TRY(plan_sieve(h, h->table, lo, hi, tlog, nth, P));
+    MP_CUDA(h, h->tilesum.ensure((size_t)P.g.ntiles * sizeof(TileSum)));
+    MP_CUDA(h, h->blockacc.ensure((size_t)P.g.ntiles * 8 + 16));
+    TileArgs a;
+    fill_tile_args(h, h->table, P, a);
+    a.sums = h->tilesum.as<TileSum>();
+    MP_TRY(run_tiles(h, h->table, P, a, 0, 0, st));
+    u64 *off = h->blockacc.as<u64>();
+    tile_scan_kernel<<<1, 1024, 0, st>>>(a.sums, P.g.ntiles, off, off + P.g.ntiles);
+    MP_CUDA(h, cudaGetLastError());
+    u64 total = 0;
+    MP_CUDA(h, cudaMemcpyAsync(&total, off + P.g.ntiles, 8, cudaMemcpyDeviceToHost, st));
+    MP_CUDA(h, cudaStreamSynchronize(st));
+    const u64 odd_total = total;
+    const int has2 = lo <= 2 && 2 < hi;
+    *count = odd_total + has2;
+    if (*count > cap || *count == 0) return MP_OK;   // caller re-sizes
+    u64 *dst = d_primes;
+    if (has2) {
+        const u64 two = 2;
+        MP_CUDA(h, cudaMemcpyAsync(d_primes, &two, 8, cudaMemcpyHostToDevice, st));
+        dst = d_primes + 1;
+    }
+    a.emit_off = off;
+    a.emit64 = dst;
+    a.emit32 = nullptr;
+    MP_TRY(run_tiles(h, h->table, P, a, 0, 1, st));
+    MP_CUDA(h, cudaStreamSynchronize(st));
+    return check_errflag(h, st);
+}

@@ -1,0 +1,87 @@
+// mp_tune.cu -- the measured autotuner: times the sieve tile geometry (bits per tile x
+// threads per CTA) and the Fermat kernel variants (limbs fixed by p, one or two primes per
+// thread) on the device with CUDA events, and keeps the fastest per handle.  The reference
+// chooses its wheel and chunk by a fitted cost model (auto_wheel / auto_chunk,
+// A350826/a350826.c:1976-2015); here the candidates are timed instead.
+#include "mp_common.cuh"
+#include <algorithm>
+
+static int time_sieve(mp_handle *h, u64 lo, u64 hi, u32 tlog, u32 nth, mp_range_stats *d_out, float *ms)
+{
+    mp_sieve_opts o;
+    memset(&o, 0, sizeof o);
+    o.mode = MP_MODE_BATCHED;
+    o.tile_log2 = tlog;
+    o.threads = nth;
+    cudaStream_t st = h->stream;
+    MP_TRY(mp_sieve_run(h, lo, hi, &o, d_out, nullptr, nullptr, nullptr, st));   // warm-up
+    MP_CUDA(h, cudaEventRecord(h->ev0, st));
+    for (int r = 0; r < 3; r++) MP_TRY(mp_sieve_run(h, lo, hi, &o, d_out, nullptr, nullptr, nullptr, st));
+    MP_CUDA(h, cudaEventRecord(h->ev1, st));
+    MP_CUDA(h, cudaEventSynchronize(h->ev1));
+    MP_CUDA(h, cudaEventElapsedTime(ms, h->ev0, h->ev1));
+    return MP_OK;
+}
+
+extern "C" int mp_autotune(mp_handle *h, uint64_t lo, char *report, size_t cap)
+{
+    if (!h) return MP_EINVAL;
+    std::lock_guard<std::recursive_mutex> lk(h->mu);
+    MP_CUDA(h, cudaSetDevice(h->device));
+    std::string rep;
+    char line[160];
+    // sieve: a range of 2^32 integers at height lo
+    const u64 span = 1ull << 32;
+    if (lo > MP_HI_MAX - span) lo = MP_HI_MAX - span;
+    MP_CUDA(h, h->small_out.ensure(4096));
+    mp_range_stats *d_out = (mp_range_stats *)h->small_out.p;
+    float best = 1e30f;
+    u32 bt = 20, bn = 1024;
+    static const u32 tl[3] = {18, 19, 20}, th[3] = {256, 512, 1024};
+    for (u32 a : tl)
+        for (u32 b : th) {
+            float ms = 0;
+            const int r = time_sieve(h, lo, lo + span, a, b, d_out, &ms);
+            if (r != MP_OK) return r;
+            snprintf(line, sizeof line, "sieve tile 2^%u x %u threads: %.3f ms / 2^32\n", a, b, ms / 3);
+            rep += line;
+            if (ms < best) { best = ms; bt = a; bn = b; }
+        }
+    h->tune.sieve_tile_log2 = (int)bt;
+    h->tune.sieve_threads = (int)bn;
+    h->tune.tuned_at = lo;
+    snprintf(line, sizeof line, "sieve choice: tile 2^%u, %u threads\n", bt, bn);
+    rep += line;
+    // Fermat: 2^20 primes near max(lo, 1e12), one vs two per thread
+    u64 plo = std::max<u64>(lo, 1000000000000ull);
+    if (plo > (1ull << 62)) plo = 1ull << 40;
+    u64 n = 0;
+    MP_TRY(mp_sieve_emit_primes(h, plo, plo + (1ull << 26), nullptr, 0, &n, h->stream));
+    MP_CUDA(h, h->ferm_p.ensure((size_t)n * 8 + 8));
+    MP_CUDA(h, h->ferm_q.ensure((size_t)n * 8 + 8));
+    u64 n2 = 0;
+    MP_TRY(mp_sieve_emit_primes(h, plo, plo + (1ull << 26), h->ferm_p.as<u64>(), n, &n2, h->stream));
+    const int k4 = (plo + (1ull << 26)) >> 47 ? 1 : 0;
+    float fb = 1e30f;
+    int fv = 0;
+    for (int ilp = 0; ilp < 2; ilp++) {
+        const int v = k4 | (ilp << 1);
+        MP_TRY(mp_fermat_run(h, h->ferm_p.as<u64>(), n, h->ferm_q.as<u64>(), h->stream, v, nullptr));
+        MP_CUDA(h, cudaEventRecord(h->ev0, h->stream));
+        for (int r = 0; r < 3; r++) MP_TRY(mp_fermat_run(h, h->ferm_p.as<u64>(), n, h->ferm_q.as<u64>(), h->stream, v, nullptr));
+        MP_CUDA(h, cudaEventRecord(h->ev1, h->stream));
+        MP_CUDA(h, cudaEventSynchronize(h->ev1));
+        float ms = 0;
+        MP_CUDA(h, cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+        snprintf(line, sizeof line, "fermat %s limbs, %d prime(s)/thread: %.3f ms for %llu primes\n", k4 ? "4" : "3",
+                 ilp + 1, ms / 3, (unsigned long long)n);
+        rep += line;
+        if (ms < fb) { fb = ms; fv = v; }
+    }
+    h->tune.fermat_variant = fv & 2;
+    if (report && cap) {
+        strncpy(report, rep.c_str(), cap - 1);
+        report[cap - 1] = 0;
+    }
+    return MP_OK;
+}

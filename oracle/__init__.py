@@ -1,0 +1,203 @@
+"""oracle -- CPU checkers for the Mathpub hot path.  TEST INFRASTRUCTURE ONLY.
+
+Only tests/, __graft_entry__.smoke() and the CPU-baseline leg of bench.py import this
+package, and only to compute expected answers or CPU timings; the product (mathpub_b200)
+never does.
+
+  liboracle.so               the C restatement in mp_oracle.c (built by `make` here)
+  _ref/libref_a350826.so     the reference's own A350826/a350826.c (BPSW, sextuplet counter)
+  _ref/libref_wieferich.so   the reference's own A001220/wieferich.c (Fermat quotients)
+The _ref libraries are compiled from the reference tree by `make ref` where that tree
+exists, and travel with the repository as built files.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_A350826 = os.path.join(HERE, "_ref", "libref_a350826.so")
+REF_WIEFERICH = os.path.join(HERE, "_ref", "libref_wieferich.so")
+REFERENCE_TREE = "/root/reference"
+
+STATS_FIELDS = ["pi", "twins", "max_gap", "gap_start", "tuple6", "tuple6_cks", "first_prime", "last_prime"]
+STATS_DTYPE = np.dtype([(n, np.uint64) for n in STATS_FIELDS])
+TAIL = 1 << 16
+
+
+class Stats(C.Structure):
+    _fields_ = [(n, C.c_uint64) for n in STATS_FIELDS]
+
+    def as_dict(self):
+        return {n: int(getattr(self, n)) for n in STATS_FIELDS}
+
+
+class Wief(C.Structure):
+    _fields_ = [(n, C.c_uint64) for n in ["primes", "tests", "near", "flt", "cks", "ordered_hash", "nhits"]] + [
+        ("hits", C.c_uint64 * 16)]
+
+
+def build(ref=True):
+    """Compile liboracle.so, and the reference checkers when the reference tree exists."""
+    target = "ref" if ref and os.path.isdir(REFERENCE_TREE) else "all"
+    subprocess.run(["make", "-s", "-C", HERE, target], check=True)
+
+
+_o = None
+_ra = None
+_rw = None
+
+
+def o():
+    global _o
+    if _o is None:
+        if not os.path.exists(ORACLE_SO):
+            build(ref=False)
+        L = C.CDLL(ORACLE_SO)
+        u64, vp = C.c_uint64, C.c_void_p
+        for name, args, res in [
+            ("or_mix64", [u64], u64),
+            ("or_bpsw", [u64], C.c_int), ("or_sprp2", [u64], C.c_int), ("or_slprp", [u64], C.c_int),
+            ("or_is_prime_ref", [u64], C.c_int),
+            ("or_bpsw_batch", [vp, C.c_size_t, vp, C.c_int], None),
+            ("or_fermat_q2", [u64, vp, vp], u64),
+            ("or_fermat_batch", [vp, C.c_size_t, vp, C.c_int], None),
+            ("or_sieve_range", [u64, u64, u64, C.c_int, C.c_int, vp, vp, vp, vp, C.c_int], C.c_int),
+            ("or_primes_range", [u64, u64, vp, C.c_size_t, C.c_int], C.c_size_t),
+            ("or_wieferich_range", [u64, u64, vp, C.c_int], C.c_int),
+            ("or_fnv1a64", [vp, C.c_size_t], u64),
+        ]:
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = res
+        _o = L
+    return _o
+
+
+def have_ref():
+    return os.path.exists(REF_A350826) and os.path.exists(REF_WIEFERICH)
+
+
+def ra():
+    global _ra
+    if _ra is None:
+        L = C.CDLL(REF_A350826)
+        u64, vp = C.c_uint64, C.c_void_p
+        for name, args, res in [("ref_bpsw", [u64], C.c_int), ("ref_sprp2_64", [u64], C.c_int),
+                                ("ref_slprp64", [u64], C.c_int), ("ref_is_prime", [u64], C.c_int),
+                                ("ref_bpsw_batch", [vp, C.c_size_t, vp, C.c_int], None),
+                                ("ref_count_sext", [u64, u64, C.c_int, vp, vp], C.c_int)]:
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = res
+        _ra = L
+    return _ra
+
+
+def rw():
+    global _rw
+    if _rw is None:
+        L = C.CDLL(REF_WIEFERICH)
+        u64, vp = C.c_uint64, C.c_void_p
+        for name, args, res in [("ref_fermat_q2", [u64, vp, vp], u64),
+                                ("ref_fermat_batch", [vp, C.c_size_t, vp, C.c_int], None),
+                                ("ref_wieferich_scan", [u64, u64, C.c_int, vp, vp, vp], C.c_int)]:
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = res
+        _rw = L
+    return _rw
+
+
+def threads():
+    return max(1, os.cpu_count() or 1)
+
+
+# ---- convenience wrappers ----
+
+def bpsw(n, nthreads=None):
+    n = np.ascontiguousarray(n, dtype=np.uint64)
+    bits = np.zeros((len(n) + 7) // 8 + 8, dtype=np.uint8)
+    o().or_bpsw_batch(n.ctypes.data, len(n), bits.ctypes.data, nthreads or threads())
+    return np.unpackbits(bits, bitorder="little")[: len(n)].astype(bool)
+
+
+def ref_bpsw(n, nthreads=None):
+    n = np.ascontiguousarray(n, dtype=np.uint64)
+    bits = np.zeros((len(n) + 7) // 8 + 8, dtype=np.uint8)
+    ra().ref_bpsw_batch(n.ctypes.data, len(n), bits.ctypes.data, nthreads or threads())
+    return np.unpackbits(bits, bitorder="little")[: len(n)].astype(bool)
+
+
+def fermat_q(p, nthreads=None):
+    p = np.ascontiguousarray(p, dtype=np.uint64)
+    q = np.zeros(len(p), dtype=np.uint64)
+    o().or_fermat_batch(p.ctypes.data, len(p), q.ctypes.data, nthreads or threads())
+    return q
+
+
+def ref_fermat_q(p, nthreads=None):
+    p = np.ascontiguousarray(p, dtype=np.uint64)
+    q = np.zeros(len(p), dtype=np.uint64)
+    rw().ref_fermat_batch(p.ctypes.data, len(p), q.ctypes.data, nthreads or threads())
+    return q
+
+
+def sieve_range(lo, hi, block_log2=0, hash_log2=0, bitmap=False, nthreads=None):
+    st = Stats()
+    nb = ((hi - lo - 1) >> block_log2) + 1 if block_log2 else 0
+    base = lo & ~1
+    nbits = (hi - base) >> 1
+    nh = (nbits + (1 << (hash_log2 - 1)) - 1) >> (hash_log2 - 1) if hash_log2 else 0
+    blocks = np.zeros(nb, dtype=STATS_DTYPE) if block_log2 else None
+    hashes = np.zeros(nh, dtype=np.uint64) if hash_log2 else None
+    bm = np.zeros((nbits + 63) // 64, dtype=np.uint64) if bitmap else None
+    rc = o().or_sieve_range(lo, hi, TAIL, block_log2, hash_log2, C.byref(st),
+                            None if blocks is None else blocks.ctypes.data,
+                            None if hashes is None else hashes.ctypes.data,
+                            None if bm is None else bm.ctypes.data, nthreads or threads())
+    if rc != 0:
+        raise RuntimeError(f"or_sieve_range failed: {rc}")
+    r = st.as_dict()
+    if blocks is not None:
+        r["blocks"] = blocks
+    if hashes is not None:
+        r["hashes"] = hashes
+    if bm is not None:
+        r["bitmap"] = bm
+    return r
+
+
+def primes_range(lo, hi, nthreads=None):
+    cap = max(16, (hi - lo) // 2 + 16)
+    out = np.zeros(cap, dtype=np.uint64)
+    n = o().or_primes_range(lo, hi, out.ctypes.data, cap, nthreads or threads())
+    return out[:n]
+
+
+def wieferich_range(lo, hi, nthreads=None):
+    w = Wief()
+    rc = o().or_wieferich_range(lo, hi, C.byref(w), nthreads or threads())
+    if rc != 0:
+        raise RuntimeError("or_wieferich_range failed")
+    d = {n: int(getattr(w, n)) for n in ["primes", "tests", "near", "flt", "cks", "ordered_hash", "nhits"]}
+    d["hits"] = [int(w.hits[i]) for i in range(min(16, d["nhits"]))]
+    return d
+
+
+def ref_count_sext(lo, hi, nthreads=None):
+    c, k = C.c_uint64(), C.c_uint64()
+    ra().ref_count_sext(lo, hi, nthreads or threads(), C.byref(c), C.byref(k))
+    return int(c.value), int(k.value)
+
+
+def ref_wieferich_scan(lo, hi, nthreads=None):
+    p, k, f = C.c_uint64(), C.c_uint64(), C.c_uint64()
+    rw().ref_wieferich_scan(lo, hi, nthreads or threads(), C.byref(p), C.byref(k), C.byref(f))
+    return int(p.value), int(k.value), int(f.value)
+
+
+def mix64(z):
+    return int(o().or_mix64(z))
