@@ -137,7 +137,10 @@ def run_ours(args):
     dev = torch.device("cuda", local)
     e = mp.Engine(local)
     L = mp.lib()
-    stream = torch.cuda.current_stream()
+    # a stream of our own (the legacy default stream has handle 0, which the library reads
+    # as "the handle's stream"); every launch and every timing event goes on it
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(stream)
     sp = stream.cuda_stream
 
     lo = LO + rank * SPAN

@@ -180,13 +180,14 @@ int mp_autotune(mp_handle *h, uint64_t lo, char *report, size_t cap);
  * bpsw_plain, fermat, fermat_stats" in that order, the launch counts and summed device
  * milliseconds since the previous read.
  * mp_probe_peaks measures device-wide rates (operations per second): shared-memory atomicOr
- * with the lanes of a warp on distinct banks and on random words, and 32-bit integer
- * multiply-adds.  These are the roofline denominators of the sieve and the Montgomery kernels.
+ * with the lanes of a warp on distinct banks and on random words, 32-bit integer
+ * multiply-adds, and global atomicOr on random words of a 64 MB buffer (the L2 atomic rate).
+ * These are the roofline denominators of the sieve and the Montgomery kernels.
  */
 int mp_profile_enable(mp_handle *h, int on);
 int mp_profile_read(mp_handle *h, uint64_t *launches, double *ms, int ncat);
 int mp_probe_peaks(mp_handle *h, double *smem_atomic_conflict_free, double *smem_atomic_random,
-                   double *imad32);
+                   double *imad32, double *l2_atomic_random);
 
 /* ---- serving (continuous batching) ----
  * Requests of two kinds: range queries [lo, hi) -> pi, max gap (+ start), twins; and

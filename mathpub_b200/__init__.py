@@ -92,7 +92,7 @@ def lib():
             "mp_autotune": ([vp, u64, C.c_char_p, C.c_size_t], C.c_int),
             "mp_profile_enable": ([vp, C.c_int], C.c_int),
             "mp_profile_read": ([vp, vp, vp, C.c_int], C.c_int),
-            "mp_probe_peaks": ([vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)], C.c_int),
+            "mp_probe_peaks": ([vp] + [C.POINTER(C.c_double)] * 4, C.c_int),
             "mp_serve_open": ([vp, vp, C.POINTER(vp)], C.c_int),
             "mp_serve_submit_range": ([vp, u64, u64, C.POINTER(u64)], C.c_int),
             "mp_serve_submit_bpsw": ([vp, vp, u32, vp, C.POINTER(u64)], C.c_int),
@@ -246,9 +246,10 @@ class Engine:
         return {c: (int(la[i]), float(ms[i])) for i, c in enumerate(self.PROF_CATS)}
 
     def probe_peaks(self):
-        a, b, c = C.c_double(), C.c_double(), C.c_double()
-        self._check(lib().mp_probe_peaks(self._h, C.byref(a), C.byref(b), C.byref(c)))
-        return {"smem_atomic_conflict_free": a.value, "smem_atomic_random": b.value, "imad32": c.value}
+        a, b, c, d = C.c_double(), C.c_double(), C.c_double(), C.c_double()
+        self._check(lib().mp_probe_peaks(self._h, C.byref(a), C.byref(b), C.byref(c), C.byref(d)))
+        return {"smem_atomic_conflict_free": a.value, "smem_atomic_random": b.value, "imad32": c.value,
+                "l2_atomic_random": d.value}
 
     def autotune(self, lo=10**15):
         buf = C.create_string_buffer(4096)

@@ -37,6 +37,7 @@ struct GraphEntry {
     GraphKey key;
     cudaGraphExec_t exec = nullptr;
     u64 stamp = 0;
+    u64 gen = 0;                     // buffer generation the graph's pointers belong to
 };
 
 struct GraphCache {
@@ -82,6 +83,10 @@ int mp_init(int device, mp_handle **out)
         return MP_ECUDA;
     }
     h->graphs = new GraphCache();
+    DevBuf *bufs[] = {&h->tilesum, &h->blockacc, &h->rec, &h->reccnt, &h->queue, &h->errflag, &h->scratch_bitmap,
+                      &h->bpsw_n, &h->bpsw_bits, &h->ferm_p, &h->ferm_q, &h->ferm_part, &h->stats_out, &h->small_out,
+                      &h->boot.q, &h->boot.magic, &h->table.q, &h->table.magic, &h->scat_bounds};
+    for (DevBuf *b : bufs) b->gen = &h->buf_gen;
     *out = h;
     return MP_OK;
 }
@@ -94,7 +99,7 @@ int mp_free(mp_handle *h)
     mp_graphs_free(h);
     DevBuf *bufs[] = {&h->tilesum, &h->blockacc, &h->rec, &h->reccnt, &h->queue, &h->errflag, &h->scratch_bitmap,
                       &h->bpsw_n, &h->bpsw_bits, &h->ferm_p, &h->ferm_q, &h->ferm_part, &h->stats_out, &h->small_out,
-                      &h->boot.q, &h->boot.magic, &h->table.q, &h->table.magic};
+                      &h->boot.q, &h->boot.magic, &h->table.q, &h->table.magic, &h->scat_bounds};
     for (DevBuf *b : bufs) b->release();
     for (int p = 0; p < MP_NPAT; p++)
         if (h->pat_ready && h->pat.d_words[p]) cudaFree(h->pat.d_words[p]);
@@ -152,7 +157,7 @@ int mp_sieve_range_dev(mp_handle *h, uint64_t lo, uint64_t hi, const mp_sieve_op
     key.bitmap = d_bitmap; key.st = st;
     GraphCache *gc = h->graphs;
     for (auto &g : gc->e)
-        if (g.exec && g.key == key) {
+        if (g.exec && g.key == key && g.gen == h->buf_gen) {
             g.stamp = ++gc->clock;
             MP_CUDA(h, cudaGraphLaunch(g.exec, st));
             return MP_OK;
@@ -163,10 +168,11 @@ int mp_sieve_range_dev(mp_handle *h, uint64_t lo, uint64_t hi, const mp_sieve_op
     MP_CUDA(h, cudaStreamIsCapturing(st, &cs));
     if (cs != cudaStreamCaptureStatusNone) return MP_OK;   // the caller is capturing
     cudaGraph_t graph = nullptr;
+    const u64 gen0 = h->buf_gen;
     MP_CUDA(h, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     const int r = mp_sieve_run(h, lo, hi, &o, d_out, d_blocks, d_hash, d_bitmap, st);
     const cudaError_t ce = cudaStreamEndCapture(st, &graph);
-    if (r != MP_OK || ce != cudaSuccess || !graph) {
+    if (r != MP_OK || ce != cudaSuccess || !graph || h->buf_gen != gen0) {
         if (graph) cudaGraphDestroy(graph);
         cudaGetLastError();
         return MP_OK;   // the direct run above already produced the results
@@ -186,6 +192,7 @@ int mp_sieve_range_dev(mp_handle *h, uint64_t lo, uint64_t hi, const mp_sieve_op
         slot->exec = exec;
         slot->key = key;
         slot->stamp = ++gc->clock;
+        slot->gen = gen0;
     } else cudaGetLastError();
     return MP_OK;
 }

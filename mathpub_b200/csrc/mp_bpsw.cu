@@ -15,14 +15,14 @@
 //
 // Two launch structures:
 //   plain    one launch per candidate list, one thread per candidate, all phases inline;
-//   batched  one persistent launch over every list: CTAs pop chunks of 2048 candidates from
-//            a device work queue, trial-divide, compact the survivors in shared memory, run
+//   batched  one persistent launch over every list: warps pop chunks of 1024 candidates from
+//            a device work queue, trial-divide, compact the survivors with warp ballots, run
 //            the base-2 test on them, compact the passers, run the Lucas test, and write the
-//            verdict words.  Compaction keeps the warps' lanes on uniform work.
+//            verdict words.  Compaction keeps the lanes on uniform work; warps never wait for
+//            one another.
 #include "mp_common.cuh"
 
 #define TD_N 30            // odd primes 3..127
-#define BPSW_CHUNK 2048
 
 __constant__ u64 c_td_inv[TD_N];
 __constant__ u64 c_td_lim[TD_N];
@@ -223,57 +223,73 @@ __global__ void __launch_bounds__(256) bpsw_plain_kernel(const u64 *__restrict__
     if ((threadIdx.x & 31) == 0 && i < len) bits[i >> 5] = b;
 }
 
-// ---- batched form: persistent CTAs over chunks of the concatenated lists ----
-__global__ void __launch_bounds__(256) bpsw_batched_kernel(const u64 *__restrict__ n, u64 total,
-                                                            u32 *__restrict__ bits, u32 *queue)
+// ---- batched form: persistent warps over chunks of the concatenated lists ----
+// Each warp pops chunks of BPSW_WCHUNK candidates from the device work queue and runs the
+// three phases on them with ballot compaction in between, so its lanes stay on uniform work;
+// warps never wait for each other (no CTA barrier).
+#define BPSW_WCHUNK 1024
+#define BPSW_WARPS 8
+
+__global__ void __launch_bounds__(BPSW_WARPS * 32) bpsw_batched_kernel(const u64 *__restrict__ n, u64 total,
+                                                                       u32 *__restrict__ bits, u32 *queue)
 {
-    __shared__ u64 s_n[BPSW_CHUNK];
-    __shared__ u16 s_idx[BPSW_CHUNK];
-    __shared__ u16 s_idx2[BPSW_CHUNK];
-    __shared__ u32 s_bits[BPSW_CHUNK / 32];
-    __shared__ u32 s_cnt[2];
-    __shared__ u32 s_chunk;
-    const u32 tid = threadIdx.x, nth = blockDim.x;
-    const u64 nchunks = (total + BPSW_CHUNK - 1) / BPSW_CHUNK;
+    __shared__ u16 s_idx[BPSW_WARPS][BPSW_WCHUNK];
+    __shared__ u32 s_bits[BPSW_WARPS][BPSW_WCHUNK / 32];
+    const u32 lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const u32 lt = (1u << lane) - 1;
+    u16 *idx = s_idx[warp];
+    u32 *wb = s_bits[warp];
+    const u64 nchunks = (total + BPSW_WCHUNK - 1) / BPSW_WCHUNK;
     for (;;) {
-        if (tid == 0) {
-            s_chunk = atomicAdd(queue, 1u);
-            s_cnt[0] = s_cnt[1] = 0;
-        }
-        for (u32 w = tid; w < BPSW_CHUNK / 32; w += nth) s_bits[w] = 0;
-        __syncthreads();
-        const u32 c = s_chunk;
+        u32 c = 0;
+        if (lane == 0) c = atomicAdd(queue, 1u);
+        c = __shfl_sync(0xffffffffu, c, 0);
         if (c >= nchunks) break;
-        const u64 c0 = (u64)c * BPSW_CHUNK;
-        const u32 len = (u32)(total - c0 < BPSW_CHUNK ? total - c0 : BPSW_CHUNK);
-        // 1. trial division; undecided candidates are compacted
-        for (u32 i = tid; i < len; i += nth) {
-            const u64 x = __ldg(n + c0 + i);
-            s_n[i] = x;
-            const int v = td_verdict(x);
-            if (v == 1) atomicOr(&s_bits[i >> 5], 1u << (i & 31));
-            else if (v < 0) s_idx[atomicAdd(&s_cnt[0], 1u)] = (u16)i;
+        const u64 c0 = (u64)c * BPSW_WCHUNK;
+        const u32 len = (u32)(total - c0 < BPSW_WCHUNK ? total - c0 : BPSW_WCHUNK);
+        const u64 *nc = n + c0;
+        // 1. trial division; verdict words for the decided candidates, survivors compacted
+        u32 ns = 0;
+        for (u32 base = 0; base < len; base += 32) {
+            const u32 i = base + lane;
+            const u64 x = i < len ? __ldg(nc + i) : 0;
+            const int v = i < len ? td_verdict(x) : 0;
+            const u32 pm = __ballot_sync(0xffffffffu, v == 1);
+            const u32 um = __ballot_sync(0xffffffffu, v < 0);
+            if (lane == 0) wb[base >> 5] = pm;
+            if (v < 0) idx[ns + __popc(um & lt)] = (u16)i;
+            ns += __popc(um);
         }
-        __syncthreads();
-        // 2. base-2 strong test on the survivors; passers are compacted
-        const u32 ns = s_cnt[0];
-        for (u32 k = tid; k < ns; k += nth) {
-            const u32 i = s_idx[k];
-            const u64 x = s_n[i];
-            if (sprp2_dev(x, m_inv(x), m_one(x))) s_idx2[atomicAdd(&s_cnt[1], 1u)] = (u16)i;
+        __syncwarp();
+        // 2. base-2 strong test on the survivors; passers compacted to the front of idx
+        u32 nl = 0;
+        for (u32 base = 0; base < ns; base += 32) {
+            const u32 k = base + lane;
+            const bool act = k < ns;
+            const u32 i = act ? idx[k] : 0;
+            bool pass = false;
+            if (act) {
+                const u64 x = __ldg(nc + i);
+                pass = sprp2_dev(x, m_inv(x), m_one(x));
+            }
+            const u32 m = __ballot_sync(0xffffffffu, pass);   // every lane has read idx[k]
+            if (pass) idx[nl + __popc(m & lt)] = (u16)i;
+            nl += __popc(m);
+            __syncwarp();
         }
-        __syncthreads();
         // 3. strong Lucas test on the base-2 passers
-        const u32 nl = s_cnt[1];
-        for (u32 k = tid; k < nl; k += nth) {
-            const u32 i = s_idx2[k];
-            const u64 x = s_n[i];
-            if (slprp_dev(x, m_inv(x), m_one(x))) atomicOr(&s_bits[i >> 5], 1u << (i & 31));
+        for (u32 base = 0; base < nl; base += 32) {
+            const u32 k = base + lane;
+            if (k < nl) {
+                const u32 i = idx[k];
+                const u64 x = __ldg(nc + i);
+                if (slprp_dev(x, m_inv(x), m_one(x))) atomicOr(&wb[i >> 5], 1u << (i & 31));
+            }
         }
-        __syncthreads();
+        __syncwarp();
         const u32 nw = (len + 31) / 32;
-        for (u32 w = tid; w < nw; w += nth) bits[(c0 >> 5) + w] = s_bits[w];
-        __syncthreads();
+        for (u32 w = lane; w < nw; w += 32) bits[(c0 >> 5) + w] = wb[w];
+        __syncwarp();
     }
 }
 
@@ -327,13 +343,14 @@ int mp_bpsw_run(mp_handle *h, const u64 *d_n, const u64 *offs, const u32 *lens, 
     MP_CUDA(h, h->queue.ensure(64));
     MP_CUDA(h, cudaMemsetAsync(h->queue.p, 0, 4, st));
     int per_sm = 0;
-    MP_CUDA(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bpsw_batched_kernel, 256, 0));
+    MP_CUDA(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bpsw_batched_kernel, BPSW_WARPS * 32, 0));
     if (per_sm < 1) per_sm = 1;
     u64 grid = (u64)h->sm_count * per_sm;
-    const u64 nchunks = (total + BPSW_CHUNK - 1) / BPSW_CHUNK;
-    if (grid > nchunks) grid = nchunks;
+    const u64 nchunks = (total + BPSW_WCHUNK - 1) / BPSW_WCHUNK;
+    const u64 need = (nchunks + BPSW_WARPS - 1) / BPSW_WARPS;
+    if (grid > need) grid = need;
     ProfScope ps(h, PROF_BPSW_BATCHED, st);
-    bpsw_batched_kernel<<<(unsigned)grid, 256, 0, st>>>(d_n, total, d_bits, h->queue.as<u32>());
+    bpsw_batched_kernel<<<(unsigned)grid, BPSW_WARPS * 32, 0, st>>>(d_n, total, d_bits, h->queue.as<u32>());
     MP_CUDA(h, cudaGetLastError());
     return MP_OK;
 }

@@ -63,7 +63,7 @@ __device__ __forceinline__ u64 mp_first_odd_multiple(u64 x0, u32 q, u32 r, u64 c
     if (r == 0) j = 0;
     else {
         const u32 d = q - r;                       // x0 + d = 0 mod q
-        j = (d & 1) ? (u64)((d + q) >> 1) : (u64)(d >> 1);
+        j = (d & 1) ? (((u64)d + q) >> 1) : (u64)(d >> 1);   // 64-bit: q may exceed 2^31
     }
     const u64 qq = (u64)q * q;
     if (qq > x0) {
@@ -77,20 +77,28 @@ __device__ __forceinline__ u64 mp_first_odd_multiple(u64 x0, u32 q, u32 r, u64 c
 // handle
 // ---------------------------------------------------------------------------------------
 
-// grow-only device buffer
+// grow-only device buffer; every reallocation bumps *gen (the handle's buffer generation),
+// which invalidates CUDA graphs captured with the old pointers
 struct DevBuf {
     void *p = nullptr;
     size_t bytes = 0;
+    u64 *gen = nullptr;
     cudaError_t ensure(size_t need)
     {
         if (need <= bytes && p) return cudaSuccess;
         if (p) { cudaFree(p); p = nullptr; bytes = 0; }
+        if (gen) (*gen)++;
         size_t b = need < 256 ? 256 : need;
         cudaError_t e = cudaMalloc(&p, b);
         if (e == cudaSuccess) bytes = b;
         return e;
     }
-    void release() { if (p) cudaFree(p); p = nullptr; bytes = 0; }
+    void release()
+    {
+        if (p) { cudaFree(p); if (gen) (*gen)++; }
+        p = nullptr;
+        bytes = 0;
+    }
     template <class T> T *as() const { return (T *)p; }
 };
 
@@ -111,6 +119,7 @@ struct PrimeTable {
     DevBuf q;                        // u32[n]
     DevBuf magic;                    // u64[n] floor((2^64-1)/q)
     std::vector<u32> host;
+    std::vector<double> inv_prefix;  // inv_prefix[i] = sum of 1/q over the first i primes
     u64 count_le(u64 x) const;       // number of table primes <= x
 };
 
@@ -148,12 +157,15 @@ struct mp_handle {
 
     // scratch
     DevBuf tilesum, blockacc, rec, reccnt, queue, errflag, scratch_bitmap, bpsw_n, bpsw_bits,
-        ferm_p, ferm_q, ferm_part, stats_out, small_out;
+        ferm_p, ferm_q, ferm_part, stats_out, small_out, scat_bounds;
+    u64 scat_key[3] = {~0ull, ~0ull, ~0ull};   // (first, end, blocks) the bounds were built for
+    u32 scat_nblk = 0;
     u32 *h_err = nullptr;            // pinned mirror of errflag
 
     Autotune tune;
     GraphCache *graphs = nullptr;
 
+    u64 buf_gen = 0;                 // bumped by every scratch reallocation
     bool prof_on = false;
     std::vector<ProfEv> prof;
     std::vector<cudaEvent_t> prof_pool;

@@ -37,6 +37,17 @@ __global__ void __launch_bounds__(1024) imad_probe(u32 iters, u32 a, u32 *sink)
     if (s == 0x12345678u) atomicAdd(sink, 1u);
 }
 
+// global atomicOr (no return value) on random words of a buffer of `words` u32 (a power of 2);
+// with a buffer well inside the L2 this is the L2 atomic rate
+__global__ void __launch_bounds__(256) l2_atomic_probe(u32 *buf, u32 mask, u32 iters)
+{
+    u32 x = (blockIdx.x * blockDim.x + threadIdx.x) * 2654435761u + 12345u;
+    for (u32 i = 0; i < iters; i++) {
+        x = x * 1664525u + 1013904223u;
+        atomicOr(buf + ((x >> 3) & mask), 1u << (x & 31));
+    }
+}
+
 extern "C" {
 
 int mp_profile_enable(mp_handle *h, int on)
@@ -69,7 +80,7 @@ int mp_profile_read(mp_handle *h, uint64_t *launches, double *ms, int ncat)
 
 // rates in operations per second over the whole device: shared atomicOr with lanes on
 // distinct banks, shared atomicOr on random addresses, 32-bit integer multiply-adds
-int mp_probe_peaks(mp_handle *h, double *smem_atomic_cf, double *smem_atomic_rand, double *imad)
+int mp_probe_peaks(mp_handle *h, double *smem_atomic_cf, double *smem_atomic_rand, double *imad, double *l2_atomic)
 {
     if (!h) return MP_EINVAL;
     std::lock_guard<std::recursive_mutex> lk(h->mu);
@@ -96,6 +107,22 @@ int mp_probe_peaks(mp_handle *h, double *smem_atomic_cf, double *smem_atomic_ran
         }
         const double ops = k < 2 ? (double)h->sm_count * 1024.0 * it : (double)h->sm_count * 2 * 1024.0 * it * 8;
         r[k] = ops / (ms * 1e-3);
+    }
+    // L2 atomics: 2^24 words (64 MB) of scratch
+    if (l2_atomic) {
+        const u32 words = 1u << 24, iters = 1u << 10;
+        MP_CUDA(h, h->scratch_bitmap.ensure((size_t)words * 4));
+        MP_CUDA(h, cudaMemsetAsync(h->scratch_bitmap.p, 0, (size_t)words * 4, st));
+        const int grid = h->sm_count * 8;
+        for (int rep = 0; rep < 2; rep++) {
+            MP_CUDA(h, cudaEventRecord(h->ev0, st));
+            l2_atomic_probe<<<grid, 256, 0, st>>>(h->scratch_bitmap.as<u32>(), words - 1, iters);
+            MP_CUDA(h, cudaGetLastError());
+            MP_CUDA(h, cudaEventRecord(h->ev1, st));
+            MP_CUDA(h, cudaEventSynchronize(h->ev1));
+            MP_CUDA(h, cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+        }
+        *l2_atomic = (double)grid * 256.0 * iters / (ms * 1e-3);
     }
     if (smem_atomic_cf) *smem_atomic_cf = r[0];
     if (smem_atomic_rand) *smem_atomic_rand = r[1];

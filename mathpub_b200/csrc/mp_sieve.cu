@@ -162,12 +162,18 @@ __device__ __forceinline__ void presieve(u32 *sm, const TileArgs &a, const u32 *
     const u32 tid = threadIdx.x, nth = blockDim.x;
     for (u32 w4 = tid * 4; w4 < NW; w4 += nth * 4) {
         u32 o0 = 0, o1 = 0, o2 = 0, o3 = 0;
+        uint4 LO[MP_NPAT], HI[MP_NPAT];
+#pragma unroll
+        for (int p = 0; p < MP_NPAT; p++) {          // all loads first: ten in flight per thread
+            const u32 a4 = ((s_off[p] >> 5) + w4) & ~3u;
+            LO[p] = __ldg((const uint4 *)(a.pat[p] + a4));
+            HI[p] = __ldg((const uint4 *)(a.pat[p] + a4 + 4));
+        }
 #pragma unroll
         for (int p = 0; p < MP_NPAT; p++) {
             const u32 bit = s_off[p] + w4 * 32;
-            const u32 s = bit >> 5, sh = bit & 31, a4 = s & ~3u;
-            const uint4 lo = __ldg((const uint4 *)(a.pat[p] + a4));
-            const uint4 hi = __ldg((const uint4 *)(a.pat[p] + a4 + 4));
+            const u32 s = bit >> 5, sh = bit & 31;
+            const uint4 lo = LO[p], hi = HI[p];
             u32 v0, v1, v2, v3, v4;
             switch (s & 3) {          // uniform across the CTA for a given tile and pattern
             case 0: v0 = lo.x; v1 = lo.y; v2 = lo.z; v3 = lo.w; v4 = hi.x; break;
@@ -245,54 +251,139 @@ __global__ void __launch_bounds__(1024) tile_kernel(TileArgs a)
         if (a.rec) {
             u32 n = __ldg(a.reccnt + rel);
             if (n > a.reccap) n = a.reccap;
-            const u32 *R = a.rec + (u64)rel * a.reccap;
-            for (u32 i = tid; i < n; i += nth) {
-                const u32 j = __ldg(R + i);
+            const u32 *R = a.rec + (u64)rel * a.reccap;       // reccap is a multiple of 4
+            const uint4 *R4 = (const uint4 *)R;
+            const u32 n4 = n >> 2;
+            u32 i = tid;
+            for (; i + 3 * nth < n4; i += 4 * nth) {             // 16 records in flight per thread
+                const uint4 r0 = __ldg(R4 + i), r1 = __ldg(R4 + i + nth);
+                const uint4 r2 = __ldg(R4 + i + 2 * nth), r3 = __ldg(R4 + i + 3 * nth);
+                const u32 js[16] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w,
+                                    r2.x, r2.y, r2.z, r2.w, r3.x, r3.y, r3.z, r3.w};
+#pragma unroll
+                for (int k = 0; k < 16; k++) atomicOr(&sm[js[k] >> 5], 1u << (js[k] & 31));
+            }
+            for (; i < n4; i += nth) {
+                const uint4 r0 = __ldg(R4 + i);
+                atomicOr(&sm[r0.x >> 5], 1u << (r0.x & 31));
+                atomicOr(&sm[r0.y >> 5], 1u << (r0.y & 31));
+                atomicOr(&sm[r0.z >> 5], 1u << (r0.z & 31));
+                atomicOr(&sm[r0.w >> 5], 1u << (r0.w & 31));
+            }
+            for (u32 k = (n4 << 2) + tid; k < n; k += nth) {
+                const u32 j = __ldg(R + k);
                 atomicOr(&sm[j >> 5], 1u << (j & 31));
             }
         }
         __syncthreads();
 
-        // 5. scans: thread `tid` owns words [w0, w1) of the tile
-        const u32 wpt = TW / nth;
-        const u32 w0 = tid * wpt;
+        // 5. scans
         if (!EMIT) {
-            Part P;
-            part_init(P);
-            for (u32 w = w0; w < w0 + wpt; w++) {
-                const u64 bit0 = G + 32ull * w;
-                const u32 vm = bits_mask(bit0, nbx), lm = bits_mask(bit0, limit);
-                const u32 pw = ~sm[w] & vm;
-                const u32 pn = ~sm[w + 1] & bits_mask(bit0 + 32, nbx);
-                const u32 pin = pw & lm;
-                const u64 x = (u64)pw | ((u64)pn << 32);
-                P.count += __popc(pin);
-                P.twins += __popc(pin & (u32)(x >> 1));
-                u32 tup = pin & (u32)((x >> 2) & (x >> 3) & (x >> 5) & (x >> 6) & (x >> 8));
-                if (tup) {
-                    P.tuples += __popc(tup);
-                    while (tup) {
-                        const u32 b = __ffs(tup) - 1;
-                        tup &= tup - 1;
-                        P.cks += mp_mix64(base + 2 * (bit0 + b) + 1);
+            // Warp w scans words [w * wpw, (w + 1) * wpw) in rows of 128 words; in a row, lane l
+            // holds words 4l .. 4l + 3 (one 16-byte load, no bank conflicts).  Positions are
+            // bits relative to the tile.  The prime before a lane's first prime is the last
+            // prime of an earlier lane of the row (a max-scan) or of an earlier row (carry).
+            const u32 wpw = TW / nwarps;
+            const u32 wbase = warp * wpw;
+            const u32 NONE32 = 0xffffffffu;
+            u32 cnt = 0, tw = 0, tu = 0;
+            u64 cks = 0;
+            u32 first = NONE32, last = NONE32, lastin = NONE32, bg = 0, bs = NONE32, carry = NONE32;
+            const u64 lim_rel = limit > G ? limit - G : 0;         // bits of the tile below limit
+            const u64 nbx_rel = nbx > G ? nbx - G : 0;
+            for (u32 r = 0; r < wpw; r += 128) {
+                const u32 w = wbase + r + 4 * lane;
+                const uint4 v = *(const uint4 *)&sm[w];
+                u32 p[5];
+                p[0] = ~v.x; p[1] = ~v.y; p[2] = ~v.z; p[3] = ~v.w;
+                u32 nx = __shfl_down_sync(0xffffffffu, p[0], 1);
+                if (lane == 31) nx = ~sm[w + 4];
+                p[4] = nx;
+                const u32 b0 = w * 32;
+                if ((u64)b0 + 160 > nbx_rel) {
+#pragma unroll
+                    for (int k = 0; k < 5; k++) p[k] &= bits_mask((u64)b0 + 32 * k, nbx_rel);
+                }
+                u32 lm[4] = {~0u, ~0u, ~0u, ~0u};
+                if ((u64)b0 + 128 > lim_rel) {
+#pragma unroll
+                    for (int k = 0; k < 4; k++) lm[k] = bits_mask((u64)b0 + 32 * k, lim_rel);
+                }
+                u32 lf = NONE32, ll = NONE32;
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    const u32 pk = p[k], pin = pk & lm[k];
+                    cnt += __popc(pin);
+                    tw += __popc(pin & __funnelshift_r(pk, p[k + 1], 1));
+                    u32 tup = pin & __funnelshift_r(pk, p[k + 1], 2) & __funnelshift_r(pk, p[k + 1], 3) &
+                              __funnelshift_r(pk, p[k + 1], 5) & __funnelshift_r(pk, p[k + 1], 6) &
+                              __funnelshift_r(pk, p[k + 1], 8);
+                    if (tup) {
+                        tu += __popc(tup);
+                        while (tup) {
+                            const u32 b = __ffs(tup) - 1;
+                            tup &= tup - 1;
+                            cks += mp_mix64(base + 2 * (G + b0 + 32 * k + b) + 1);
+                        }
+                    }
+                    if (pin) lastin = b0 + 32 * k + 31 - __clz(pin);
+                    u32 y = pk;
+                    while (y) {                              // gaps inside the lane's 128 bits
+                        const u32 pos = b0 + 32 * k + __ffs(y) - 1;
+                        y &= y - 1;
+                        if (ll == NONE32) lf = pos;
+                        else if ((u64)ll < lim_rel) {
+                            const u32 g = pos - ll;
+                            if (g > bg || (g == bg && ll < bs)) { bg = g; bs = ll; }
+                        }
+                        ll = pos;
                     }
                 }
-                u32 y = pw;
-                while (y) {
-                    const u32 b = __ffs(y) - 1;
-                    y &= y - 1;
-                    const u64 pos = bit0 + b;
-                    if (P.last == MP_NONE) P.first = pos;
-                    else if (P.last < limit) {
-                        const u32 g = (u32)(pos - P.last);
-                        if (g > P.mg) { P.mg = g; P.mgs = P.last; }
-                    }
-                    P.last = pos;
-                    if (pos < limit) P.lastin = pos;
+                // last prime before this lane's first: inclusive max-scan of (last + 1)
+                u32 sc = ll == NONE32 ? 0u : ll + 1;
+#pragma unroll
+                for (int d = 1; d < 32; d <<= 1) {
+                    const u32 u = __shfl_up_sync(0xffffffffu, sc, d);
+                    if (lane >= (u32)d && u > sc) sc = u;
                 }
+                u32 ex = __shfl_up_sync(0xffffffffu, sc, 1);
+                if (lane == 0) ex = 0;
+                const u32 prev = ex ? ex - 1 : carry;
+                if (lf != NONE32 && prev != NONE32 && (u64)prev < lim_rel) {
+                    const u32 g = lf - prev;
+                    if (g > bg || (g == bg && prev < bs)) { bg = g; bs = prev; }
+                }
+                const u32 rowlast = __shfl_sync(0xffffffffu, sc, 31);
+                if (rowlast) carry = rowlast - 1;
+                if (first == NONE32 && lf != NONE32) first = lf;
+                if (ll != NONE32) last = ll;
             }
-            P = part_warp_reduce(P, limit);
-            if (lane == 0) s_part[warp] = P;
+            // warp reduction (sums, min first, max last / lastin, widest gap with the smallest
+            // start), then the warps join in order
+#pragma unroll
+            for (int d = 16; d >= 1; d >>= 1) {
+                cnt += __shfl_xor_sync(0xffffffffu, cnt, d);
+                tw += __shfl_xor_sync(0xffffffffu, tw, d);
+                tu += __shfl_xor_sync(0xffffffffu, tu, d);
+                cks += __shfl_xor_sync(0xffffffffu, cks, d);
+                first = min(first, __shfl_xor_sync(0xffffffffu, first, d));
+                const u32 ol = __shfl_xor_sync(0xffffffffu, last, d);
+                last = (last == NONE32) ? ol : (ol == NONE32 ? last : max(last, ol));
+                const u32 oi = __shfl_xor_sync(0xffffffffu, lastin, d);
+                lastin = (lastin == NONE32) ? oi : (oi == NONE32 ? lastin : max(lastin, oi));
+                const u32 og = __shfl_xor_sync(0xffffffffu, bg, d), os = __shfl_xor_sync(0xffffffffu, bs, d);
+                if (og > bg || (og == bg && os < bs)) { bg = og; bs = os; }
+            }
+            if (lane == 0) {
+                Part P;
+                P.count = cnt; P.twins = tw; P.tuples = tu; P.cks = cks;
+                P.first = first == NONE32 ? MP_NONE : G + first;
+                P.last = last == NONE32 ? MP_NONE : G + last;
+                P.lastin = lastin == NONE32 ? MP_NONE : G + lastin;
+                P.mg = bs == NONE32 ? 0 : bg;
+                P.mgs = bs == NONE32 ? MP_NONE : G + bs;
+                s_part[warp] = P;
+            }
             __syncthreads();
             if (warp == 0) {
                 Part Q;
@@ -316,7 +407,10 @@ __global__ void __launch_bounds__(1024) tile_kernel(TileArgs a)
                 }
             }
         } else {
-            // emit: in-range primes in order; per-thread counts, then a CTA-wide scan
+            // emit: in-range primes in order; thread `tid` owns words [w0, w0 + wpt); per-thread
+            // counts, then a CTA-wide scan
+            const u32 wpt = TW / nth;
+            const u32 w0 = tid * wpt;
             u32 c = 0;
             for (u32 w = w0; w < w0 + wpt; w++) c += __popc(~sm[w] & bits_mask(G + 32ull * w, limit));
             u32 incl = c;
@@ -365,8 +459,7 @@ struct ScatterArgs {
     u64 nbx;
     const u32 *q;
     const u64 *magic;
-    u32 i0, i1;                      // prime index range (large primes)
-    u32 ppb;                         // primes per CTA
+    const u32 *bounds;               // CTA b takes primes [bounds[b], bounds[b + 1])
     u32 *rec;                        // [wt][cap]
     u32 *cnt;                        // [wt], zeroed before the launch
     u32 cap;
@@ -376,18 +469,59 @@ struct ScatterArgs {
 // every hit j of prime q in the wave (plus the first HALO_BITS bits after it): record
 // (tile, offset) for its own tile, and (tile - 1, offset + 2^TLOG) when it lies in the first
 // HALO_BITS bits of a tile, because the previous tile sieves those bits as its halo
+// The hits of a prime in the wave are j0 + m q.  They are walked four at a time: the four
+// slot atomics are issued before the four record stores, so several atomics are in flight per
+// thread.  Lanes walk in lock step: lanes of a warp that hit the same tile take neighbouring
+// slots, which keeps their record stores together.
 template <int PASS>
-__device__ __forceinline__ void scatter_prime(const ScatterArgs &a, u32 k, u64 x0, u64 wstart, u64 wend_halo,
-                                              u32 *scnt, const u32 *sbase)
+__device__ __forceinline__ void scatter_halo(const ScatterArgs &a, u32 tl, u32 off, u32 *scnt, const u32 *sbase)
+{
+    // a hit in the first HALO_BITS bits of tile tl is also a record of tile tl - 1 (its halo)
+    if (off < HALO_BITS && tl >= 1 && tl - 1 < a.wt) {
+        if (PASS == 0) atomicAdd(&scnt[tl - 1], 1u);
+        else {
+            const u32 slot = sbase[tl - 1] + atomicAdd(&scnt[tl - 1], 1u);
+            if (slot < a.cap) a.rec[(u64)(tl - 1) * a.cap + slot] = off + (1u << a.tlog);
+            else atomicOr(a.err, 2u);
+        }
+    }
+}
+
+template <int PASS>
+__device__ __forceinline__ void scatter_prime(const ScatterArgs &a, u32 k, u64 x0, u32 span, u32 *scnt, const u32 *sbase)
 {
     const u32 q = __ldg(a.q + k);
     const u32 r = mp_mod_barrett(x0, q, __ldg(a.magic + k));
-    u64 j = wstart + mp_first_odd_multiple(x0, q, r, wend_halo - wstart);
-    const u32 T = 1u << a.tlog;
-    for (; j < wend_halo; j += q) {
-        const u32 tl = (u32)(j >> a.tlog) - a.t0;    // tile relative to the wave
-        const u32 off = (u32)j & (T - 1);
-        if (tl < a.wt) {
+    const u64 j64 = mp_first_odd_multiple(x0, q, r, span);
+    if (j64 >= span) return;
+    const u32 j0 = (u32)j64;                           // bit relative to the wave (tile aligned)
+    const u32 H = (span - 1 - j0) / q + 1;             // hits in [j0, span)
+    const u32 tlog = a.tlog, tmask = (1u << tlog) - 1, wt = a.wt;
+    u32 m = 0, j = j0;
+    for (; m + 4 <= H; m += 4, j += 4 * q) {
+        u32 jj[4], tl[4], sl[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) { jj[u] = j + u * q; tl[u] = jj[u] >> tlog; }
+        if (PASS == 0) {
+#pragma unroll
+            for (int u = 0; u < 4; u++) if (tl[u] < wt) atomicAdd(&scnt[tl[u]], 1u);
+        } else {
+#pragma unroll
+            for (int u = 0; u < 4; u++) sl[u] = tl[u] < wt ? sbase[tl[u]] + atomicAdd(&scnt[tl[u]], 1u) : 0;
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                if (tl[u] < wt) {
+                    if (sl[u] < a.cap) a.rec[(u64)tl[u] * a.cap + sl[u]] = jj[u] & tmask;
+                    else atomicOr(a.err, 2u);
+                }
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) scatter_halo<PASS>(a, tl[u], jj[u] & tmask, scnt, sbase);
+    }
+    for (; m < H; m++, j += q) {
+        const u32 tl = j >> tlog, off = j & tmask;
+        if (tl < wt) {
             if (PASS == 0) atomicAdd(&scnt[tl], 1u);
             else {
                 const u32 slot = sbase[tl] + atomicAdd(&scnt[tl], 1u);
@@ -395,14 +529,7 @@ __device__ __forceinline__ void scatter_prime(const ScatterArgs &a, u32 k, u64 x
                 else atomicOr(a.err, 2u);
             }
         }
-        if (off < HALO_BITS && tl >= 1 && tl - 1 < a.wt) {
-            if (PASS == 0) atomicAdd(&scnt[tl - 1], 1u);
-            else {
-                const u32 slot = sbase[tl - 1] + atomicAdd(&scnt[tl - 1], 1u);
-                if (slot < a.cap) a.rec[(u64)(tl - 1) * a.cap + slot] = off + T;
-                else atomicOr(a.err, 2u);
-            }
-        }
+        scatter_halo<PASS>(a, tl, off, scnt, sbase);
     }
 }
 
@@ -419,10 +546,9 @@ __global__ void __launch_bounds__(512) scatter_kernel(ScatterArgs a)
     u64 wend_halo = wend + HALO_BITS;
     if (wend_halo > a.nbx) wend_halo = a.nbx;
     const u64 x0 = a.base + 2 * wstart + 1;
-    const u32 k0 = a.i0 + blockIdx.x * a.ppb;
-    u32 k1 = k0 + a.ppb;
-    if (k1 > a.i1) k1 = a.i1;
-    for (u32 k = k0 + tid; k < k1; k += nth) scatter_prime<0>(a, k, x0, wstart, wend_halo, scnt, sbase);
+    const u32 k0 = __ldg(a.bounds + blockIdx.x), k1 = __ldg(a.bounds + blockIdx.x + 1);
+    const u32 span = (u32)(wend_halo - wstart);        // < 2^31 (checked by the planner)
+    for (u32 k = k0 + tid; k < k1; k += nth) scatter_prime<0>(a, k, x0, span, scnt, sbase);
     __syncthreads();
     for (u32 i = tid; i < a.wt; i += nth) {
         const u32 c = scnt[i];
@@ -430,7 +556,7 @@ __global__ void __launch_bounds__(512) scatter_kernel(ScatterArgs a)
         scnt[i] = 0;
     }
     __syncthreads();
-    for (u32 k = k0 + tid; k < k1; k += nth) scatter_prime<1>(a, k, x0, wstart, wend_halo, scnt, sbase);
+    for (u32 k = k0 + tid; k < k1; k += nth) scatter_prime<1>(a, k, x0, span, scnt, sbase);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -783,7 +909,7 @@ static u32 bucket_cap(u32 tlog, u64 qmax)
     double s = qmax > (u64)a ? log(log((double)qmax) / log(a)) : 0.0;
     double e = T * s * 1.06 + 8.0 * sqrt(T * s + 1.0) + 4096.0;
     if (e > 4.0e9) e = 4.0e9;
-    return (u32)e;
+    return ((u32)e + 3) & ~3u;
 }
 
 struct SievePlan {
@@ -811,11 +937,14 @@ static int plan_sieve(mp_handle *h, const PrimeTable &tb, u64 lo, u64 hi, u32 tl
     if (P.large) {
         const u64 qmax = tb.host[P.ti.iend - 1];
         P.cap = bucket_cap(tlog, qmax);
-        // wave: at most 64 MB of records per wave and at most 256 tiles
-        u64 wt = (64ull << 20) / ((u64)P.cap * 4);
+        // wave: enough tiles to keep every SM busy for several tiles (8 per SM), within
+        // 2 GB of records
+        u64 wt = 8ull * (u64)h->sm_count;
+        const u64 wmem = (2048ull << 20) / ((u64)P.cap * 4);
+        if (wt > wmem) wt = wmem;
         if (wt < 1) wt = 1;
-        if (wt > 256) wt = 256;
         if (wt > P.g.ntiles) wt = P.g.ntiles;
+        while (wt > 1 && (wt << tlog) + HALO_BITS >= (1ull << 31)) wt /= 2;   // 32-bit wave positions
         P.wt = (u32)wt;
         P.nwaves = (P.g.ntiles + P.wt - 1) / P.wt;
     } else {
@@ -834,6 +963,34 @@ static void fill_tile_args(mp_handle *h, const PrimeTable &tb, const SievePlan &
     for (int p = 0; p < MP_NPAT; p++) { a.pat[p] = h->pat.d_words[p]; a.period[p] = h->pat.period[p]; }
 }
 
+// CTA boundaries for the scatter kernel: contiguous runs of the large primes [i0, i1) with
+// equal shares of the sum of 1/q (the expected hits per wave), so that the CTAs of the small
+// large primes, which hit far more often, get proportionally fewer primes.  Built on the host
+// from the table's prefix sums and uploaded once per prime range (never inside a capture).
+static int scatter_bounds(mp_handle *h, const PrimeTable &tb, u32 i0, u32 i1)
+{
+    const u32 want = (u32)std::max<u64>(1, std::min<u64>((u64)h->sm_count * 16, i1 - i0));
+    if (h->scat_key[0] == i0 && h->scat_key[1] == i1 && h->scat_key[2] == want && h->scat_nblk) return MP_OK;
+    std::vector<u32> b;
+    b.reserve(want + 1);
+    b.push_back(i0);
+    const double p0 = tb.inv_prefix[i0], p1 = tb.inv_prefix[i1];
+    for (u32 c = 1; c < want; c++) {
+        const double target = p0 + (p1 - p0) * c / want;
+        u32 k = (u32)(std::lower_bound(tb.inv_prefix.begin() + i0, tb.inv_prefix.begin() + i1, target) -
+                      tb.inv_prefix.begin());
+        if (k <= b.back()) k = b.back() + 1;
+        if (k >= i1) break;
+        b.push_back(k);
+    }
+    b.push_back(i1);
+    MP_CUDA(h, h->scat_bounds.ensure(b.size() * 4));
+    MP_CUDA(h, cudaMemcpy(h->scat_bounds.p, b.data(), b.size() * 4, cudaMemcpyHostToDevice));
+    h->scat_key[0] = i0; h->scat_key[1] = i1; h->scat_key[2] = want;
+    h->scat_nblk = (u32)b.size() - 1;
+    return MP_OK;
+}
+
 // mode: 0 batched (waves of persistent tile launches), 1 plain (one launch per tile)
 static int run_tiles(mp_handle *h, const PrimeTable &tb, const SievePlan &P, TileArgs a, int mode, int emit,
                      cudaStream_t st)
@@ -848,6 +1005,7 @@ static int run_tiles(mp_handle *h, const PrimeTable &tb, const SievePlan &P, Til
         MP_CUDA(h, h->rec.ensure((size_t)wt * P.cap * 4));
         MP_CUDA(h, h->reccnt.ensure((size_t)wt * 4 * 2));
     }
+    if (P.large) MP_TRY(scatter_bounds(h, tb, P.ti.it1, P.ti.iend));
     const int grid_pers = h->sm_count * tile_ctas_per_sm(P.g.tlog, nth);
     for (u32 L = 0; L < nlaunch; L++) {
         const u32 t0 = mode == 1 ? L : L * P.wt;
@@ -856,11 +1014,10 @@ static int run_tiles(mp_handle *h, const PrimeTable &tb, const SievePlan &P, Til
             ScatterArgs s;
             s.base = P.g.base; s.tlog = P.g.tlog; s.t0 = t0; s.wt = nt; s.nbx = P.g.nbx;
             s.q = tb.q.as<u32>(); s.magic = tb.magic.as<u64>();
-            s.i0 = P.ti.it1; s.i1 = P.ti.iend;
-            s.ppb = 2048;
+            s.bounds = h->scat_bounds.as<u32>();
             s.rec = h->rec.as<u32>(); s.cnt = h->reccnt.as<u32>(); s.cap = P.cap; s.err = errp;
             MP_CUDA(h, cudaMemsetAsync(s.cnt, 0, (size_t)nt * 4, st));
-            const u32 nblk = (P.ti.iend - P.ti.it1 + s.ppb - 1) / s.ppb;
+            const u32 nblk = h->scat_nblk;
             {
                 ProfScope ps(h, PROF_SCATTER, st);
                 scatter_kernel<<<nblk, 512, (size_t)nt * 8, st>>>(s);
@@ -949,6 +1106,10 @@ int mp_tables_ensure(mp_handle *h, u64 limit)
     h->table.host.resize(total);
     MP_CUDA(h, cudaMemcpyAsync(h->table.host.data(), h->table.q.p, (size_t)total * 4, cudaMemcpyDeviceToHost, st));
     MP_CUDA(h, cudaStreamSynchronize(st));
+    h->table.inv_prefix.resize(total + 1);
+    h->table.inv_prefix[0] = 0.0;
+    for (u64 i = 0; i < total; i++) h->table.inv_prefix[i + 1] = h->table.inv_prefix[i] + 1.0 / h->table.host[i];
+    h->scat_key[0] = ~0ull;
     MP_TRY(check_errflag(h, st));
     h->table.n = total;
     h->table.limit = L;

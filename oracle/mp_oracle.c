@@ -482,17 +482,20 @@ static void sieve_part(void *cp, size_t a, size_t b)
     const u64 base = x->base;
     const u64 WB = 1 << 20;                               /* bits per window */
     u64 *next = (u64 *)malloc((x->np ? x->np : 1) * sizeof *next);
-    /* first odd multiple >= the first number of the part, at least q^2 */
+    /* bit index of the first odd multiple >= the first number of the part, at least q^2;
+       kept as an offset from x0 so that nothing overflows near 2^64 */
     const u64 x0 = base + 2 * (u64)a + 1;
     size_t np = 0;
     const u64 xend = base + 2 * (u64)b + 1;
     for (size_t k = 0; k < x->np; k++) {
         const u64 q = x->pr[k];
         if ((u128)q * q >= xend) break;
-        u64 r = x0 % q, m = r ? x0 + (q - r) : x0;
-        if (!(m & 1)) m += q;
-        if (m < q * q) m = q * q;
-        next[k] = (m - base - 1) >> 1;                    /* bit index */
+        const u64 r = x0 % q;
+        u64 d = r ? q - r : 0;                            /* x0 + d is a multiple of q */
+        if (d & 1) d += q;                                /* ... and odd */
+        u64 j = a + d / 2;
+        if (q * q > x0) j = a + (q * q - x0) / 2;
+        next[k] = j;
         np = k + 1;
     }
     for (u64 w0 = a; w0 < b; w0 += WB) {

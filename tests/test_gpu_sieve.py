@@ -139,3 +139,15 @@ def test_errors_are_reported(engine):
         engine.sieve_range(0, 100, tile_log2=17)
     # the handle still works afterwards
     assert engine.sieve_range(0, 100)["pi"] == 25
+
+
+def test_graph_replay_after_buffer_growth(engine):
+    """A batched call is captured as a CUDA graph and replayed when it repeats; a larger call in
+    between reallocates the scratch buffers, which must retire the older graph."""
+    a = (10 ** 12, 10 ** 12 + 2 ** 24)
+    first = engine.sieve_range(*a, block_log2=22, hash_log2=18)
+    engine.sieve_range(10 ** 13, 10 ** 13 + 2 ** 33, block_log2=24, hash_log2=22)
+    for _ in range(3):
+        again = engine.sieve_range(*a, block_log2=22, hash_log2=18)
+        assert same(first, again)
+        assert np.array_equal(first["blocks"], again["blocks"]) and np.array_equal(first["hashes"], again["hashes"])

@@ -150,3 +150,14 @@ def test_config_fixtures_consistent(configs):
 def test_mix64_matches_reference_definition(orc):
     for z in [0, 1, 2 ** 63, 2 ** 64 - 1, 12345678901234567]:
         assert orc.mix64(z) == mix64(z)
+
+
+def test_sieve_near_2_64_against_bpsw(orc):
+    """Near the top of the range every sieving prime is close to 2^32: the sieve must agree
+    with BPSW run on every odd number."""
+    lo = 2 ** 64 - 2 ** 26
+    odd = np.arange(lo + 1, lo + 1 + 2 * 300000, 2, dtype=np.uint64)
+    r = orc.sieve_range(lo, lo + 600001, bitmap=True)
+    v = orc.bpsw(odd)
+    bits = np.unpackbits(r["bitmap"].view(np.uint8), bitorder="little")[: len(odd)].astype(bool)
+    assert np.array_equal(bits, v) and r["pi"] == int(v.sum())
