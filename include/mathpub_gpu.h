@@ -166,6 +166,20 @@ typedef struct {
 
 int mp_wieferich_range(mp_handle *h, uint64_t lo, uint64_t hi, mp_wief_stats *out);
 
+/* The statistics that mp_wieferich_range reports, for device arrays of primes d_p[0..count)
+ * and their quotients d_q (as mp_fermat_q_base2_dev writes them), into d_stats in device
+ * memory (`primes` there = count), queued on `stream` (NULL = the legacy default stream).
+ * For callers that cannot allocate device memory -- a framework whose allocator owns the
+ * whole device, or a loop where a cudaMalloc, which may synchronise, is not allowed -- it
+ * allocates nothing and takes no handle.  Its scratch is a fixed array of about 3 MB inside
+ * the library that every device holds until exit and that all calls on a device share:
+ * calls that overlap on the GPU race.  count above MP_NOALLOC_MAX_COUNT is refused with
+ * MP_EINVAL.  The first call on a device looks up the array's device address; make that
+ * call before any stream capture.  This entry point has no counterpart in the reference. */
+#define MP_NOALLOC_MAX_COUNT (1u << 24)
+int mp_wieferich_stats_noalloc(const uint64_t *d_p, const uint64_t *d_q, uint64_t count,
+                               mp_wief_stats *d_stats, void *stream);
+
 /* ---- autotuner ----
  * Times the sieve tile geometry (tile bits x threads) on a short range at height `lo`
  * and the Fermat kernel variants, and keeps the fastest per handle.  Called implicitly

@@ -89,6 +89,7 @@ def lib():
             "mp_fermat_q_base2": ([vp, vp, C.c_size_t, vp], C.c_int),
             "mp_fermat_q_base2_dev": ([vp, vp, C.c_size_t, vp, vp], C.c_int),
             "mp_wieferich_range": ([vp, u64, u64, vp], C.c_int),
+            "mp_wieferich_stats_noalloc": ([vp, vp, u64, vp, vp], C.c_int),
             "mp_autotune": ([vp, u64, C.c_char_p, C.c_size_t], C.c_int),
             "mp_profile_enable": ([vp, C.c_int], C.c_int),
             "mp_profile_read": ([vp, vp, vp, C.c_int], C.c_int),

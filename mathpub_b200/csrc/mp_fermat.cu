@@ -279,3 +279,80 @@ int mp_fermat_reduce(mp_handle *h, const u64 *d_p, const u64 *d_q, u64 count, mp
     MP_CUDA(h, cudaGetLastError());
     return MP_OK;
 }
+
+// ---------------------------------------------------------------------------------------
+// mp_wieferich_stats_noalloc: the statistics of mp_wieferich_range for caller-supplied device
+// arrays of primes and quotients, for callers that must not allocate device memory -- code
+// that runs under a memory manager or pool that owns the whole device, inside a framework
+// whose allocator may not be bypassed, or in a latency-critical loop where a cudaMalloc
+// (which can synchronise the device) is not allowed.  It uses no handle (a handle allocates
+// its tables and buffers) and no allocation of any kind: its scratch lives in the file-scope
+// array below, which every GPU that loads this library keeps until the process exits.
+// ---------------------------------------------------------------------------------------
+
+#define NOALLOC_MAX_COUNT (1u << 24)                       // primes per call
+#define NOALLOC_PARTS (NOALLOC_MAX_COUNT / 256)           // one partial per 256-thread CTA
+
+struct NoallocScratch {
+    FermPart parts[NOALLOC_PARTS];                          // 3 MB
+    u64 hits[16];
+    u64 nhits;
+};
+
+static __device__ __align__(256) NoallocScratch g_noalloc_scratch;
+
+// The host sees g_noalloc_scratch only as a stand-in symbol: its device address is looked up
+// once per device with cudaGetSymbolAddress (with that device current) and kept here.
+static std::mutex g_noalloc_mu;
+static void *g_noalloc_ptr[64] = {nullptr};
+
+__global__ void noalloc_clear_kernel(NoallocScratch *s)
+{
+    if (threadIdx.x < 16) s->hits[threadIdx.x] = 0;
+    if (threadIdx.x == 0) s->nhits = 0;
+}
+
+// the entry count, and the stored hits in increasing order (the order in which the device
+// found them is arbitrary)
+__global__ void noalloc_finish_kernel(mp_wief_stats *out, u64 count)
+{
+    out->primes = count;
+    const int n = out->nhits < 16 ? (int)out->nhits : 16;
+    for (int i = 1; i < n; i++) {
+        const u64 v = out->hits[i];
+        int k = i - 1;
+        while (k >= 0 && out->hits[k] > v) { out->hits[k + 1] = out->hits[k]; k--; }
+        out->hits[k + 1] = v;
+    }
+}
+
+extern "C" int mp_wieferich_stats_noalloc(const uint64_t *d_p, const uint64_t *d_q, uint64_t count,
+                                           mp_wief_stats *d_stats, void *stream)
+{
+    if (!d_stats || (count && (!d_p || !d_q))) return MP_EINVAL;
+    if (count > NOALLOC_MAX_COUNT) return MP_EINVAL;       // beyond the fixed scratch
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return MP_ECUDA;
+    NoallocScratch *s = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        if (!g_noalloc_ptr[dev]) {
+            void *p = nullptr;
+            if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return MP_ECUDA;
+            g_noalloc_ptr[dev] = p;
+        }
+        s = (NoallocScratch *)g_noalloc_ptr[dev];
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    // the hit list carries over from the previous call: it must start at zero
+    noalloc_clear_kernel<<<1, 32, 0, st>>>(s);
+    const u64 nb = count ? (count + 255) / 256 : 0;
+    if (count) fermat_stats_kernel<<<(unsigned)nb, 256, 0, st>>>(d_p, d_q, count, s->parts, s->hits, &s->nhits);
+    else {
+        // no input: one empty partial
+        if (cudaMemsetAsync(s->parts, 0, sizeof(FermPart), st) != cudaSuccess) return MP_ECUDA;
+    }
+    fermat_final_kernel<<<1, 1024, 0, st>>>(s->parts, nb ? nb : 1, &s->nhits, s->hits, d_stats);
+    noalloc_finish_kernel<<<1, 1, 0, st>>>(d_stats, count);
+    return cudaGetLastError() == cudaSuccess ? MP_OK : MP_ECUDA;
+}
