@@ -216,7 +216,7 @@ typedef struct {
     uint64_t mem_budget;    /* bytes of device memory for in-flight requests (0 = auto) */
     uint32_t max_inflight;  /* requests admitted at once (0 = 256) */
     uint32_t streams;       /* device streams that overlap batches (0 = 4) */
-    uint64_t prime_limit;   /* resident sieving primes up to this bound (0 = 2^32 - 1) */
+    uint64_t prime_limit;   /* resident sieving primes up to this bound (0 = 2^30: heights to ~1.15e18) */
 } mp_serve_opts;
 
 typedef struct {

@@ -53,6 +53,17 @@ class WiefStats(C.Structure):
 STATS_DTYPE = np.dtype([(n, np.uint64) for n in STATS_FIELDS])
 
 
+class ServeOpts(C.Structure):
+    _fields_ = [("mem_budget", C.c_uint64), ("max_inflight", C.c_uint32), ("streams", C.c_uint32),
+                ("prime_limit", C.c_uint64)]
+
+
+class ServeResult(C.Structure):
+    _fields_ = [("kind", C.c_uint32), ("status", C.c_int32), ("pi", C.c_uint64), ("max_gap", C.c_uint64),
+                ("gap_start", C.c_uint64), ("twins", C.c_uint64), ("count", C.c_uint32),
+                ("submit_s", C.c_double), ("done_s", C.c_double)]
+
+
 class MathpubError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"{_ERRNAMES.get(code, code)}: {msg}")
@@ -256,3 +267,59 @@ class Engine:
         buf = C.create_string_buffer(4096)
         self._check(lib().mp_autotune(self._h, lo, buf, 4096))
         return buf.value.decode()
+
+
+class Server:
+    """Continuous-batching request server on an Engine (mp_serve_*)."""
+
+    def __init__(self, engine, streams=4, max_inflight=256, mem_budget=0, prime_limit=0):
+        self.e = engine
+        self._s = C.c_void_p()
+        o = ServeOpts(mem_budget, max_inflight, streams, prime_limit)
+        engine._check(lib().mp_serve_open(engine.handle, C.byref(o), C.byref(self._s)))
+        self._bits = {}
+
+    def submit_range(self, lo, hi):
+        rid = C.c_uint64()
+        rc = lib().mp_serve_submit_range(self._s, lo, hi, C.byref(rid))
+        if rc != MP_OK:
+            raise MathpubError(rc, f"submit_range({lo}, {hi})")
+        return rid.value
+
+    def submit_bpsw(self, n):
+        n = np.ascontiguousarray(n, dtype=np.uint64)
+        bits = np.zeros((len(n) + 7) // 8 + 8, dtype=np.uint8)
+        rid = C.c_uint64()
+        rc = lib().mp_serve_submit_bpsw(self._s, _p(n), len(n), _p(bits), C.byref(rid))
+        if rc != MP_OK:
+            raise MathpubError(rc, "submit_bpsw")
+        self._bits[rid.value] = (bits, len(n))
+        return rid.value
+
+    def poll(self, rid, wait_ms=0):
+        """None while pending; else a dict (range: pi, max_gap, gap_start, twins; primality:
+        'verdicts' bool array) with 'submit_s', 'done_s' and 'status'."""
+        r = ServeResult()
+        rc = lib().mp_serve_poll(self._s, rid, C.byref(r), wait_ms)
+        if rc == MP_EAGAIN:
+            return None
+        if rc != MP_OK:
+            raise MathpubError(rc, f"poll({rid})")
+        d = {"kind": r.kind, "status": r.status, "submit_s": r.submit_s, "done_s": r.done_s}
+        if r.kind == 1:
+            d.update(pi=int(r.pi), max_gap=int(r.max_gap), gap_start=int(r.gap_start), twins=int(r.twins))
+        else:
+            bits, n = self._bits.pop(rid)
+            d["verdicts"] = np.unpackbits(bits, bitorder="little")[:n].astype(bool)
+        return d
+
+    def close(self):
+        if self._s:
+            lib().mp_serve_close(self._s)
+            self._s = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

@@ -102,7 +102,7 @@ int mp_free(mp_handle *h)
                       &h->boot.q, &h->boot.magic, &h->table.q, &h->table.magic, &h->scat_bounds};
     for (DevBuf *b : bufs) b->release();
     for (int p = 0; p < MP_NPAT; p++)
-        if (h->pat_ready && h->pat.d_words[p]) cudaFree(h->pat.d_words[p]);
+        if (!h->shared_tables && h->pat_ready && h->pat.d_words[p]) cudaFree(h->pat.d_words[p]);
     if (h->h_err) cudaFreeHost(h->h_err);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
@@ -147,7 +147,8 @@ int mp_sieve_range_dev(mp_handle *h, uint64_t lo, uint64_t hi, const mp_sieve_op
     memset(&o, 0, sizeof o);
     if (opts) o = *opts;
     if (o.hash_log2 && !d_hash) return mp_set_error(h, MP_EINVAL, "hash_log2 set but no hash buffer");
-    if (o.mode == MP_MODE_PLAIN || h->prof_on) return mp_sieve_run(h, lo, hi, &o, d_out, d_blocks, d_hash, d_bitmap, st);
+    if (o.mode == MP_MODE_PLAIN || h->prof_on || h->no_graphs)
+        return mp_sieve_run(h, lo, hi, &o, d_out, d_blocks, d_hash, d_bitmap, st);
     // batched: replay a captured graph of an identical earlier call.  The tables are built
     // before capture (they synchronise), so the graph holds kernel launches and memsets only.
     if (hi > lo && hi <= MP_HI_MAX) MP_TRY(mp_tables_ensure(h, mp_isqrt64(hi + MP_TAIL - 1)));

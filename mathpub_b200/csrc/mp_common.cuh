@@ -120,6 +120,7 @@ struct PrimeTable {
     DevBuf magic;                    // u64[n] floor((2^64-1)/q)
     std::vector<u32> host;
     std::vector<double> inv_prefix;  // inv_prefix[i] = sum of 1/q over the first i primes
+    std::vector<u32> work_bounds;    // prime indices cutting the table into runs of equal sum 1/q
     u64 count_le(u64 x) const;       // number of table primes <= x
 };
 
@@ -152,13 +153,18 @@ struct mp_handle {
 
     PrimeTable boot;                 // odd primes < 2^16 (bootstraps the big table)
     PrimeTable table;                // odd primes up to table.limit
+    PrimeTable *tab = &table;        // the table in use: a serving worker uses its server's
+    bool shared_tables = false;      // tab and pat belong to another handle (never rebuilt here)
     PatternSet pat;
     bool pat_ready = false;
+    bool no_graphs = false;          // run batched sieve calls directly (no capture / replay)
+    int servers_open = 0;            // servers sharing this handle's table (it may not be rebuilt)
 
     // scratch
     DevBuf tilesum, blockacc, rec, reccnt, queue, errflag, scratch_bitmap, bpsw_n, bpsw_bits,
         ferm_p, ferm_q, ferm_part, stats_out, small_out, scat_bounds;
     u64 scat_key[3] = {~0ull, ~0ull, ~0ull};   // (first, end, blocks) the bounds were built for
+    std::vector<u32> scat_host;
     u32 scat_nblk = 0;
     u32 *h_err = nullptr;            // pinned mirror of errflag
 

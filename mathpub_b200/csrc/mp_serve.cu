@@ -1,14 +1,281 @@
-// mp_serve.cu -- request serving with continuous batching (see include/mathpub_gpu.h).
+// mp_serve.cu -- request serving with continuous batching (include/mathpub_gpu.h, serving).
+//
+// A server owns K workers.  Each worker is a handle of its own (stream, scratch buffers)
+// that uses the server's resident sieving-prime table and presieve patterns, built once at
+// open for every height the server accepts.  Requests wait in one FIFO.  A worker takes
+// the next request when an in-flight slot is free and the request's device-memory estimate
+// fits in what the budget has left (admission by free device memory), so requests that
+// arrive while others are on the GPU are admitted as soon as slots and memory free up.
+//   range request      runs the batched sieve on the worker's stream; K workers overlap on
+//                      the device;
+//   primality request  a worker that picks one takes every primality request waiting at
+//                      that moment (up to a candidate cap) and runs them as ONE persistent
+//                      batched BPSW launch over all their lists (continuous batching).
+// Results are those of the same request run alone: the kernels are the same and every
+// request has its own outputs; only scheduling differs.
 #include "mp_common.cuh"
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <thread>
+#include <unordered_map>
+
+struct ServeReq {
+    u64 id = 0;
+    u32 kind = 0;                    // 1 range, 2 primality
+    u64 lo = 0, hi = 0;
+    std::vector<u64> cand;
+    u8 *out_bits = nullptr;
+    u64 mem = 0;
+    bool done = false;
+    mp_serve_result res;
+};
+
+struct mp_server {
+    mp_handle *main = nullptr;
+    std::vector<mp_handle *> workers;
+    std::vector<std::thread> threads;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<ServeReq *> pending;
+    std::unordered_map<u64, ServeReq *> reqs;
+    u64 next_id = 1;
+    bool closing = false;
+    u64 budget = 0, mem_used = 0;
+    u32 max_inflight = 256, inflight = 0;
+    u64 prime_limit = 0;
+    u64 bpsw_cap = 1ull << 22;       // candidates per merged primality launch
+};
+
+static double now_s()
+{
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+// device memory a request occupies while it runs (scratch of its launch)
+static u64 range_mem(u64 lo, u64 hi)
+{
+    const u64 bits = (hi + MP_TAIL - (lo & ~1ull)) / 2;
+    const u64 tiles = (bits >> 20) + 1;
+    const u64 wave = std::min<u64>(tiles, 1184);
+    return tiles * 64 + wave * (1ull << 20) + (1ull << 20);
+}
+
+static u64 bpsw_mem(u64 count) { return count * 8 + count / 8 + 4096; }
+
+static void run_range(mp_handle *w, ServeReq *r)
+{
+    mp_sieve_opts o;
+    memset(&o, 0, sizeof o);
+    o.mode = MP_MODE_BATCHED;
+    mp_range_stats st;
+    memset(&st, 0, sizeof st);
+    const int rc = mp_sieve_range(w, r->lo, r->hi, &o, &st, nullptr, nullptr, nullptr);
+    r->res.status = rc;
+    r->res.pi = st.pi;
+    r->res.max_gap = st.max_gap;
+    r->res.gap_start = st.gap_start;
+    r->res.twins = st.twins;
+}
+
+static void run_bpsw(mp_handle *w, std::vector<ServeReq *> &batch)
+{
+    std::vector<const uint64_t *> lists;
+    std::vector<uint32_t> lens;
+    std::vector<uint8_t *> outs;
+    for (ServeReq *r : batch) {
+        lists.push_back(r->cand.data());
+        lens.push_back((uint32_t)r->cand.size());
+        outs.push_back(r->out_bits);
+    }
+    const int rc = mp_bpsw_batches(w, lists.data(), lens.data(), (uint32_t)batch.size(), outs.data());
+    for (ServeReq *r : batch) r->res.status = rc;
+}
+
+static void worker_loop(mp_server *s, mp_handle *w)
+{
+    for (;;) {
+        std::vector<ServeReq *> take;
+        {
+            std::unique_lock<std::mutex> lk(s->mu);
+            for (;;) {
+                if (s->closing && s->pending.empty()) return;
+                if (!s->pending.empty() && s->inflight < s->max_inflight) {
+                    ServeReq *head = s->pending.front();
+                    // admission: the head always fits when nothing else holds memory
+                    if (s->mem_used + head->mem <= s->budget || s->mem_used == 0) break;
+                }
+                s->cv_work.wait_for(lk, std::chrono::milliseconds(50));
+            }
+            ServeReq *head = s->pending.front();
+            if (head->kind == 1) {
+                s->pending.pop_front();
+                take.push_back(head);
+            } else {
+                // merge every waiting primality request (in arrival order) into one launch
+                u64 cand = 0;
+                for (auto it = s->pending.begin(); it != s->pending.end();) {
+                    ServeReq *r = *it;
+                    if (r->kind == 2 && (take.empty() || (cand + r->cand.size() <= s->bpsw_cap &&
+                                                         s->mem_used + r->mem <= s->budget &&
+                                                         s->inflight + take.size() < s->max_inflight))) {
+                        cand += r->cand.size();
+                        take.push_back(r);
+                        s->mem_used += r->mem;
+                        it = s->pending.erase(it);
+                    } else ++it;
+                }
+                for (ServeReq *r : take) s->mem_used -= r->mem;   // re-added below, once
+            }
+            for (ServeReq *r : take) s->mem_used += r->mem;
+            s->inflight += (u32)take.size();
+        }
+        if (take[0]->kind == 1) run_range(w, take[0]);
+        else run_bpsw(w, take);
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            const double t = now_s();
+            for (ServeReq *r : take) {
+                r->res.done_s = t;
+                r->done = true;
+                s->mem_used -= r->mem;
+            }
+            s->inflight -= (u32)take.size();
+        }
+        s->cv_done.notify_all();
+        s->cv_work.notify_all();
+    }
+}
 
 extern "C" {
-int mp_serve_open(mp_handle *h, const mp_serve_opts *, mp_server **out)
+
+int mp_serve_open(mp_handle *h, const mp_serve_opts *opts, mp_server **out)
 {
-    if (out) *out = nullptr;
-    return mp_set_error(h, MP_EINVAL, "serving not built yet");
+    if (!h || !out) return MP_EINVAL;
+    *out = nullptr;
+    mp_serve_opts o;
+    memset(&o, 0, sizeof o);
+    if (opts) o = *opts;
+    std::lock_guard<std::recursive_mutex> lk(h->mu);
+    MP_CUDA(h, cudaSetDevice(h->device));
+    const u64 limit = o.prime_limit ? o.prime_limit : (1ull << 30);
+    // the resident table covers every height whose square root is below the limit
+    MP_TRY(mp_tables_ensure(h, limit > 0xffffffffull ? 0xffffffffull : limit));
+    mp_server *s = new mp_server();
+    s->main = h;
+    s->prime_limit = h->tab->limit;
+    size_t fr = 0, tot = 0;
+    MP_CUDA(h, cudaMemGetInfo(&fr, &tot));
+    s->budget = o.mem_budget ? o.mem_budget : (u64)fr / 2;
+    s->max_inflight = o.max_inflight ? o.max_inflight : 256;
+    const u32 k = o.streams ? o.streams : 4;
+    for (u32 i = 0; i < k; i++) {
+        mp_handle *w = nullptr;
+        int rc = mp_init(h->device, &w);
+        if (rc != MP_OK) {
+            mp_serve_close(s);
+            return mp_set_error(h, rc, "serving worker %u could not be created", i);
+        }
+        w->tab = h->tab;
+        w->shared_tables = true;
+        w->pat = h->pat;
+        w->pat_ready = true;
+        w->no_graphs = true;
+        w->tune = h->tune;
+        s->workers.push_back(w);
+    }
+    for (mp_handle *w : s->workers) s->threads.emplace_back(worker_loop, s, w);
+    h->servers_open++;
+    *out = s;
+    return MP_OK;
 }
-int mp_serve_submit_range(mp_server *, uint64_t, uint64_t, uint64_t *) { return MP_EINVAL; }
-int mp_serve_submit_bpsw(mp_server *, const uint64_t *, uint32_t, uint8_t *, uint64_t *) { return MP_EINVAL; }
-int mp_serve_poll(mp_server *, uint64_t, mp_serve_result *, int) { return MP_EINVAL; }
-int mp_serve_close(mp_server *) { return MP_EINVAL; }
+
+static int submit(mp_server *s, ServeReq *r, uint64_t *req_id)
+{
+    r->res.submit_s = now_s();
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (s->closing) { delete r; return MP_EINVAL; }
+        r->id = s->next_id++;
+        s->reqs[r->id] = r;
+        s->pending.push_back(r);
+    }
+    if (req_id) *req_id = r->id;
+    s->cv_work.notify_one();
+    return MP_OK;
 }
+
+int mp_serve_submit_range(mp_server *s, uint64_t lo, uint64_t hi, uint64_t *req_id)
+{
+    if (!s || hi <= lo || hi > MP_HI_MAX) return MP_EINVAL;
+    if (mp_isqrt64(hi + MP_TAIL - 1) > s->prime_limit) return MP_ERANGE;
+    ServeReq *r = new ServeReq();
+    memset(&r->res, 0, sizeof r->res);
+    r->kind = 1;
+    r->lo = lo;
+    r->hi = hi;
+    r->mem = range_mem(lo, hi);
+    r->res.kind = 1;
+    return submit(s, r, req_id);
+}
+
+int mp_serve_submit_bpsw(mp_server *s, const uint64_t *n, uint32_t count, uint8_t *verdict_bits, uint64_t *req_id)
+{
+    if (!s || (count && (!n || !verdict_bits)) || count > (1u << 24)) return MP_EINVAL;
+    ServeReq *r = new ServeReq();
+    memset(&r->res, 0, sizeof r->res);
+    r->kind = 2;
+    r->cand.assign(n, n + count);
+    r->out_bits = verdict_bits;
+    r->mem = bpsw_mem(count);
+    r->res.kind = 2;
+    r->res.count = count;
+    if (!count) {
+        // nothing to test: done at once
+        std::lock_guard<std::mutex> lk(s->mu);
+        r->id = s->next_id++;
+        r->done = true;
+        r->res.submit_s = r->res.done_s = now_s();
+        s->reqs[r->id] = r;
+        if (req_id) *req_id = r->id;
+        return MP_OK;
+    }
+    return submit(s, r, req_id);
+}
+
+int mp_serve_poll(mp_server *s, uint64_t req_id, mp_serve_result *res, int wait_ms)
+{
+    if (!s || !res) return MP_EINVAL;
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto it = s->reqs.find(req_id);
+    if (it == s->reqs.end()) return MP_EINVAL;
+    ServeReq *r = it->second;
+    if (!r->done && wait_ms > 0)
+        s->cv_done.wait_for(lk, std::chrono::milliseconds(wait_ms), [&] { return r->done; });
+    if (!r->done) return MP_EAGAIN;
+    *res = r->res;
+    s->reqs.erase(it);
+    delete r;
+    return MP_OK;
+}
+
+int mp_serve_close(mp_server *s)
+{
+    if (!s) return MP_EINVAL;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->closing = true;
+    }
+    s->cv_work.notify_all();
+    for (auto &t : s->threads) t.join();
+    for (mp_handle *w : s->workers) mp_free(w);
+    for (auto &kv : s->reqs) delete kv.second;
+    if (s->main && !s->threads.empty()) {
+        std::lock_guard<std::recursive_mutex> lk(s->main->mu);
+        s->main->servers_open--;
+    }
+    delete s;
+    return MP_OK;
+}
+
+}  // extern "C"

@@ -967,25 +967,49 @@ static void fill_tile_args(mp_handle *h, const PrimeTable &tb, const SievePlan &
 // equal shares of the sum of 1/q (the expected hits per wave), so that the CTAs of the small
 // large primes, which hit far more often, get proportionally fewer primes.  Built on the host
 // from the table's prefix sums and uploaded once per prime range (never inside a capture).
-static int scatter_bounds(mp_handle *h, const PrimeTable &tb, u32 i0, u32 i1)
+static int scatter_bounds(mp_handle *h, const PrimeTable &tb, u32 i0, u32 i1, cudaStream_t st)
 {
     const u32 want = (u32)std::max<u64>(1, std::min<u64>((u64)h->sm_count * 16, i1 - i0));
     if (h->scat_key[0] == i0 && h->scat_key[1] == i1 && h->scat_key[2] == want && h->scat_nblk) return MP_OK;
-    std::vector<u32> b;
-    b.reserve(want + 1);
+    std::vector<u32> &b = h->scat_host;
+    b.clear();
     b.push_back(i0);
-    const double p0 = tb.inv_prefix[i0], p1 = tb.inv_prefix[i1];
-    for (u32 c = 1; c < want; c++) {
-        const double target = p0 + (p1 - p0) * c / want;
-        u32 k = (u32)(std::lower_bound(tb.inv_prefix.begin() + i0, tb.inv_prefix.begin() + i1, target) -
-                      tb.inv_prefix.begin());
-        if (k <= b.back()) k = b.back() + 1;
-        if (k >= i1) break;
-        b.push_back(k);
+    if (!tb.work_bounds.empty()) {
+        // the table's equal-work cut points inside (i0, i1), then halve the widest runs until
+        // there are enough CTAs
+        auto a = std::upper_bound(tb.work_bounds.begin(), tb.work_bounds.end(), i0);
+        auto z = std::lower_bound(tb.work_bounds.begin(), tb.work_bounds.end(), i1);
+        for (auto it = a; it != z; ++it) b.push_back(*it);
+        b.push_back(i1);
+        while (b.size() - 1 < want) {
+            std::vector<u32> c;
+            c.push_back(b[0]);
+            bool grew = false;
+            for (size_t k = 1; k < b.size(); k++) {
+                if (b[k] - b[k - 1] >= 2 && c.size() + (b.size() - k) < (size_t)want + 1) {
+                    c.push_back(b[k - 1] + (b[k] - b[k - 1]) / 2);
+                    grew = true;
+                }
+                c.push_back(b[k]);
+            }
+            b.swap(c);
+            if (!grew) break;
+        }
+    } else {
+        const double p0 = tb.inv_prefix[i0], p1 = tb.inv_prefix[i1];
+        for (u32 c = 1; c < want; c++) {
+            const double target = p0 + (p1 - p0) * c / want;
+            u32 k = (u32)(std::lower_bound(tb.inv_prefix.begin() + i0, tb.inv_prefix.begin() + i1, target) -
+                          tb.inv_prefix.begin());
+            if (k <= b.back()) k = b.back() + 1;
+            if (k >= i1) break;
+            b.push_back(k);
+        }
+        b.push_back(i1);
     }
-    b.push_back(i1);
     MP_CUDA(h, h->scat_bounds.ensure(b.size() * 4));
-    MP_CUDA(h, cudaMemcpy(h->scat_bounds.p, b.data(), b.size() * 4, cudaMemcpyHostToDevice));
+    MP_CUDA(h, cudaMemcpyAsync(h->scat_bounds.p, b.data(), b.size() * 4, cudaMemcpyHostToDevice, st));
+    MP_CUDA(h, cudaStreamSynchronize(st));
     h->scat_key[0] = i0; h->scat_key[1] = i1; h->scat_key[2] = want;
     h->scat_nblk = (u32)b.size() - 1;
     return MP_OK;
@@ -1005,7 +1029,7 @@ static int run_tiles(mp_handle *h, const PrimeTable &tb, const SievePlan &P, Til
         MP_CUDA(h, h->rec.ensure((size_t)wt * P.cap * 4));
         MP_CUDA(h, h->reccnt.ensure((size_t)wt * 4 * 2));
     }
-    if (P.large) MP_TRY(scatter_bounds(h, tb, P.ti.it1, P.ti.iend));
+    if (P.large) MP_TRY(scatter_bounds(h, tb, P.ti.it1, P.ti.iend, st));
     const int grid_pers = h->sm_count * tile_ctas_per_sm(P.g.tlog, nth);
     for (u32 L = 0; L < nlaunch; L++) {
         const u32 t0 = mode == 1 ? L : L * P.wt;
@@ -1051,6 +1075,10 @@ static int check_errflag(mp_handle *h, cudaStream_t st)
 int mp_tables_ensure(mp_handle *h, u64 limit)
 {
     MP_TRY(mp_patterns_ensure(h));
+    if (limit <= h->tab->limit) return MP_OK;
+    if (h->shared_tables || h->servers_open)
+        return mp_set_error(h, MP_ERANGE, "needs sieving primes up to %llu, above the resident table (%llu) that "
+                            "an open server shares", (unsigned long long)limit, (unsigned long long)h->tab->limit);
     cudaStream_t st = h->stream;
     if (!h->boot.n) {
         MP_CUDA(h, h->boot.q.ensure(6600 * 4));
@@ -1069,7 +1097,6 @@ int mp_tables_ensure(mp_handle *h, u64 limit)
         MP_CUDA(h, cudaMemcpyAsync(h->boot.host.data(), h->boot.q.p, (size_t)n * 4, cudaMemcpyDeviceToHost, st));
         MP_CUDA(h, cudaStreamSynchronize(st));
     }
-    if (limit <= h->table.limit) return MP_OK;
     u64 L = std::max<u64>(limit, std::max<u64>(1ull << 22, 2 * h->table.limit));
     if (L > 0xffffffffull) L = 0xffffffffull;
     if (limit > L) return mp_set_error(h, MP_ERANGE, "sieving primes above 2^32 are not supported");
@@ -1109,6 +1136,19 @@ int mp_tables_ensure(mp_handle *h, u64 limit)
     h->table.inv_prefix.resize(total + 1);
     h->table.inv_prefix[0] = 0.0;
     for (u64 i = 0; i < total; i++) h->table.inv_prefix[i + 1] = h->table.inv_prefix[i] + 1.0 / h->table.host[i];
+    {
+        // 32768 runs of equal sum 1/q over the whole table (the scatter CTAs of any prime range
+        // are cut from these)
+        const int NB = 32768;
+        h->table.work_bounds.clear();
+        const double P = h->table.inv_prefix[total];
+        for (int c = 1; c < NB; c++) {
+            const u64 k = (u64)(std::lower_bound(h->table.inv_prefix.begin(), h->table.inv_prefix.end(), P * c / NB) -
+                                h->table.inv_prefix.begin());
+            if (k < total && (h->table.work_bounds.empty() || k > h->table.work_bounds.back()))
+                h->table.work_bounds.push_back((u32)k);
+        }
+    }
     h->scat_key[0] = ~0ull;
     MP_TRY(check_errflag(h, st));
     h->table.n = total;
@@ -1145,7 +1185,7 @@ int mp_sieve_run(mp_handle *h, u64 lo, u64 hi, const mp_sieve_opts *o, mp_range_
     const u64 top = hi + MP_TAIL;
     MP_TRY(mp_tables_ensure(h, mp_isqrt64(top - 1)));
     SievePlan P;
-    MP_TRY(plan_sieve(h, h->table, lo, hi, tlog, nth, P));
+    MP_TRY(plan_sieve(h, *h->tab, lo, hi, tlog, nth, P));
     MP_CUDA(h, h->tilesum.ensure((size_t)P.g.ntiles * sizeof(TileSum)));
     // bitmap: the caller's, or scratch when only hashes are wanted
     const u64 nwords64 = (P.g.limit + 63) >> 6;
@@ -1155,10 +1195,10 @@ int mp_sieve_run(mp_handle *h, u64 lo, u64 hi, const mp_sieve_opts *o, mp_range_
         bm = h->scratch_bitmap.as<u32>();
     }
     TileArgs a;
-    fill_tile_args(h, h->table, P, a);
+    fill_tile_args(h, *h->tab, P, a);
     a.sums = h->tilesum.as<TileSum>();
     a.bitmap32 = bm;
-    MP_TRY(run_tiles(h, h->table, P, a, (int)mode, 0, st));
+    MP_TRY(run_tiles(h, *h->tab, P, a, (int)mode, 0, st));
     // fold
     u32 tpb;
     u64 nblocks;
@@ -1210,13 +1250,13 @@ int mp_sieve_emit_primes(mp_handle *h, u64 lo, u64 hi, u64 *d_primes, u64 cap, u
     const u64 top = hi + MP_TAIL;
     MP_TRY(mp_tables_ensure(h, mp_isqrt64(top - 1)));
     SievePlan P;
-    MP_TRY(plan_sieve(h, h->table, lo, hi, tlog, nth, P));
+    MP_TRY(plan_sieve(h, *h->tab, lo, hi, tlog, nth, P));
     MP_CUDA(h, h->tilesum.ensure((size_t)P.g.ntiles * sizeof(TileSum)));
     MP_CUDA(h, h->blockacc.ensure((size_t)P.g.ntiles * 8 + 16));
     TileArgs a;
-    fill_tile_args(h, h->table, P, a);
+    fill_tile_args(h, *h->tab, P, a);
     a.sums = h->tilesum.as<TileSum>();
-    MP_TRY(run_tiles(h, h->table, P, a, 0, 0, st));
+    MP_TRY(run_tiles(h, *h->tab, P, a, 0, 0, st));
     u64 *off = h->blockacc.as<u64>();
     tile_scan_kernel<<<1, 1024, 0, st>>>(a.sums, P.g.ntiles, off, off + P.g.ntiles);
     MP_CUDA(h, cudaGetLastError());
@@ -1236,7 +1276,7 @@ int mp_sieve_emit_primes(mp_handle *h, u64 lo, u64 hi, u64 *d_primes, u64 cap, u
     a.emit_off = off;
     a.emit64 = dst;
     a.emit32 = nullptr;
-    MP_TRY(run_tiles(h, h->table, P, a, 0, 1, st));
+    MP_TRY(run_tiles(h, *h->tab, P, a, 0, 1, st));
     MP_CUDA(h, cudaStreamSynchronize(st));
     return check_errflag(h, st);
 }
