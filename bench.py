@@ -175,6 +175,8 @@ def run_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
+    # the measured autotuner picks the tile geometry at this height (and the Fermat variant)
+    tune_report = e.autotune(LO) if args.autotune else "off"
     # warm-up (builds the prime tables and captures the graph on the first call)
     for _ in range(args.warmup):
         sieve_dev()
@@ -284,10 +286,17 @@ def run_ours(args):
     peaks = e.probe_peaks()
     hbm, hbm_src = peaks_file()
 
+    fermat = run_fermat(e, world, rank) if not args.quick else None
+    serving = run_serving(e, args) if (rank == 0 and not args.quick and args.serve_requests) else None
+
     line = None
     if rank == 0:
         primes = e.primes_range(3, int(np.sqrt(float(hi + (1 << 16)))) + 2)
         tile_bits = 1 << 20
+        import re
+        m = re.search(r"sieve choice: tile 2\^(\d+)", tune_report)
+        if m:
+            tile_bits = 1 << int(m.group(1))
         marks_small, marks_large = algorithmic_work(primes, lo, hi, tile_bits)
         ntiles = -(-((hi + (1 << 16) - lo) // 2) // tile_bits)
         tile_bytes = (marks_large * 4 + ntiles * (tile_bits // 8)) / max(tile_launches, 1)
@@ -313,7 +322,7 @@ def run_ours(args):
                     "api": "mp_sieve_range (host buffers)"},
             "gpu_launches": launches_per_step * args.steps,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                         "frac": achieved / hbm, "traffic": None, "kernel": "tile_kernel<20,0>",
+                         "frac": achieved / hbm, "traffic": None, "kernel": f"tile_kernel<{tile_bits.bit_length() - 1},0>",
                          "peak_source": f"{hbm_src} (MEASURED_PEAKS.json hbm_gbs)" if hbm_src == "measured" else "fallback",
                          "algorithmic_bytes_per_launch": tile_bytes, "avg_launch_ms": tile_avg_s * 1e3,
                          "note": "bytes = bucket records read (4 B per large-prime hit) + bitmap written; "
@@ -334,6 +343,9 @@ def run_ours(args):
                      "same_verdicts": bpsw_same, "primes": bpsw_primes,
                      "workload": "2^26 seeded odd u64 (60% uniform [2^40,2^64), 30% p*q near 2^62, "
                                  "10% (k+1)(2k+1) / Chernick), 4096 lists, log-uniform lengths"},
+            "fermat": fermat,
+            "serving": serving,
+            "autotune": tune_report.strip().splitlines()[-3:] if tune_report != "off" else "off",
             "probes": peaks,
             "results": res, "results_match_fixture": (res == ref_fixture) if (ref_fixture and rank == 0 and lo == LO) else None,
             "clocks": clocks,
@@ -348,6 +360,128 @@ def run_ours(args):
         print(json.dumps(line), flush=True)
 
 
+def run_fermat(e, world, rank):
+    """Config 4: every prime in [1e12 + r 4e9, 1e12 + (r+1) 4e9) from the GPU sieve, base-2
+    Fermat quotients with the full statistics; device time of the quotient and reduction
+    kernels (events on the handle's stream), and the host-API call end to end."""
+    lo = 10 ** 12 + rank * 4 * 10 ** 9
+    hi = lo + 4 * 10 ** 9
+    e.wieferich_range(lo, hi)                         # warm-up
+    t0 = time.perf_counter()
+    r = e.wieferich_range(lo, hi)
+    wall = time.perf_counter() - t0
+    kms = e.last_kernel_ms()
+    fix = None
+    try:
+        with open(os.path.join(ROOT, "tests", "golden", "configs.json")) as f:
+            c4 = json.load(f)["config4"]
+        fix = all(r[k] == c4[k] for k in ("primes", "tests", "near", "flt", "cks", "ordered_hash")) if lo == 10 ** 12 else None
+    except Exception:
+        pass
+    return {"workload": "base-2 Fermat quotients of every prime in [1e12, 1e12+4e9) (per rank), 3-limb Montgomery",
+            "tests": r["tests"], "tests_per_s": r["tests"] / (kms / 1e3), "kernel_ms": kms,
+            "e2e_tests_per_s": r["tests"] / wall, "e2e_ms": wall * 1e3, "near": r["near"], "flt": r["flt"],
+            "cks": r["cks"], "results_match_fixture": fix}
+
+
+def run_serving(e, args):
+    """Config 5: a seeded stream of mixed requests arriving as a Poisson process.  70% range
+    queries [lo, lo+len), lo log-uniform in [1e9, 1e18], len log-uniform in [2^16, 2^32]; 30%
+    primality batches of 1..65536 candidates from the BPSW workload distribution.  The arrival
+    rate is 70% of the capacity measured by a burst; latency = completion - submission (host
+    clock).  Baseline: a sample of the same requests, each run alone with plain launches."""
+    import threading
+    import mathpub_b200 as mp
+    import torch
+    rng = np.random.default_rng(0x5E17E)
+    pool, _ = mp.bpsw_workload(0x5E17E, 1 << 22, 0)
+
+    def make(n):
+        out = []
+        for _ in range(n):
+            if rng.random() < 0.7:
+                lo = int(10 ** rng.uniform(9, 18))
+                out.append(("r", lo, lo + int(2 ** rng.uniform(16, 32))))
+            else:
+                k = int(2 ** rng.uniform(0, 16))
+                a = int(rng.integers(0, len(pool) - k))
+                out.append(("b", pool[a:a + k]))
+        return out
+
+    def work(reqs):
+        return (sum(r[2] - r[1] for r in reqs if r[0] == "r"), sum(len(r[1]) for r in reqs if r[0] == "b"))
+
+    with mp.Server(e, streams=4) as srv:
+        # capacity from a burst
+        burst = make(3000)
+        t0 = time.perf_counter()
+        ids = [srv.submit_range(r[1], r[2]) if r[0] == "r" else srv.submit_bpsw(r[1]) for r in burst]
+        for rid in ids:
+            while srv.poll(rid, wait_ms=1000) is None:
+                pass
+        cap = len(burst) / (time.perf_counter() - t0)
+        rate = 0.7 * cap
+        reqs = make(args.serve_requests)
+        arr = np.cumsum(rng.exponential(1.0 / rate, size=len(reqs)))
+        res = [None] * len(reqs)
+        ids = [None] * len(reqs)
+        ready = threading.Semaphore(0)
+
+        def poller():
+            for i in range(len(reqs)):
+                ready.acquire()
+                r = None
+                while r is None:
+                    r = srv.poll(ids[i], wait_ms=1000)
+                res[i] = r
+
+        th = threading.Thread(target=poller)
+        th.start()
+        t0 = time.perf_counter()
+        for i, r in enumerate(reqs):
+            d = arr[i] - (time.perf_counter() - t0)
+            if d > 0:
+                time.sleep(d)
+            ids[i] = srv.submit_range(r[1], r[2]) if r[0] == "r" else srv.submit_bpsw(r[1])
+            ready.release()
+        th.join()
+        span = max(x["done_s"] for x in res) - min(x["submit_s"] for x in res)
+        lat = np.array([x["done_s"] - x["submit_s"] for x in res]) * 1e3
+        bad = sum(1 for x in res if x["status"] != 0)
+    ints, tests = work(reqs)
+    # each request alone with plain launches (a sample)
+    sample = reqs[:60]
+    L = mp.lib()
+    alone = []
+    for r in sample:
+        t0 = time.perf_counter()
+        if r[0] == "r":
+            e.sieve_range(r[1], r[2], mode=mp.MODE_PLAIN)
+        else:
+            n = np.ascontiguousarray(r[1], dtype=np.uint64)
+            pad = (len(n) + 31) // 32 * 32
+            flat = np.zeros(pad, dtype=np.uint64)
+            flat[:len(n)] = n
+            dn = torch.from_numpy(flat.view(np.int64)).cuda()
+            db = torch.zeros(pad // 32 + 1, dtype=torch.int32, device="cuda")
+            offs = np.array([0, pad], dtype=np.uint64)
+            lens = np.array([len(n)], dtype=np.uint32)
+            import ctypes as C
+            L.mp_bpsw_lists_dev(e.handle, C.c_void_p(dn.data_ptr()), C.c_void_p(offs.ctypes.data),
+                                C.c_void_p(lens.ctypes.data), 1, C.c_void_p(db.data_ptr()), mp.MODE_PLAIN, None)
+            torch.cuda.synchronize()
+        alone.append(time.perf_counter() - t0)
+    alone = np.array(alone) * 1e3
+    return {"requests": len(reqs), "rate_req_per_s": rate, "burst_capacity_req_per_s": cap,
+            "throughput_req_per_s": len(reqs) / span, "ints_per_s": ints / span, "tests_per_s": tests / span,
+            "latency_ms_p50": float(np.percentile(lat, 50)), "latency_ms_p99": float(np.percentile(lat, 99)),
+            "latency_ms_mean": float(lat.mean()), "failed": bad, "streams": 4,
+            "alone_plain_sample": {"requests": len(sample), "req_per_s": len(sample) / (alone.sum() / 1e3),
+                                   "latency_ms_p50": float(np.percentile(alone, 50)),
+                                   "latency_ms_p99": float(np.percentile(alone, 99))},
+            "served_over_alone_throughput": (len(reqs) / span) / (len(sample) / (alone.sum() / 1e3))}
+
+
 def cpu_baseline(sample_log2=31):
     """The oracle's restatement of the reference's odd-only sieve (every output of the
     workload) on [1e15, 1e15 + 2^31) with all host threads."""
@@ -360,6 +494,19 @@ def cpu_baseline(sample_log2=31):
     out = {"value": (hi - lo) / dt, "unit": "ints/s", "cores": t, "kind": "port",
            "sample": f"[1e15, 1e15+2^{sample_log2}) with every output, {t} threads, {dt:.2f} s"}
     if oracle.have_ref():
+        import mathpub_b200 as mp
+        n, _ = mp.bpsw_workload(BPSW_SEED, 1 << 22, 0)
+        t0 = time.perf_counter()
+        oracle.ref_bpsw(n, t)
+        dt = time.perf_counter() - t0
+        out["bpsw"] = {"value": len(n) / dt, "unit": "tests/s", "cores": t, "kind": "reference",
+                       "sample": f"2^22 candidates of the BPSW workload, reference sprp2_64x4 + slprp64, {t} threads"}
+        p = oracle.primes_range(10 ** 12, 10 ** 12 + 4 * 10 ** 7, t)
+        t0 = time.perf_counter()
+        oracle.ref_fermat_q(p, t)
+        dt = time.perf_counter() - t0
+        out["fermat"] = {"value": len(p) / dt, "unit": "tests/s", "cores": t, "kind": "reference",
+                         "sample": f"{len(p)} primes of [1e12, 1e12+4e7), reference run_group (8 lanes), {t} threads"}
         t0 = time.perf_counter()
         oracle.ref_count_sext(lo, hi, t)
         dt = time.perf_counter() - t0
@@ -406,6 +553,9 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--serve-requests", type=int, default=100000)
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false")
+    ap.add_argument("--quick", action="store_true", help="headline sieve, plain form and BPSW only")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
