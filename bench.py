@@ -124,6 +124,7 @@ def run_ours(args):
     import torch
     import torch.distributed as dist
     import mathpub_b200 as mp
+    from mathpub_b200 import shard
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -143,8 +144,7 @@ def run_ours(args):
     torch.cuda.set_stream(stream)
     sp = stream.cuda_stream
 
-    lo = LO + rank * SPAN
-    hi = lo + SPAN
+    lo, hi = shard.weak_shard(LO, SPAN, rank)
     nb = L.mp_sieve_nblocks(lo, hi, BLOCK_LOG2)
     nh = L.mp_sieve_nhashes(lo, hi, HASH_LOG2)
     d_out = torch.zeros(8, dtype=torch.int64, device=dev)
@@ -169,11 +169,7 @@ def run_ours(args):
             torch.cuda.synchronize()
 
     def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return shard.max_over_ranks(x, device=dev)
 
     # the measured autotuner picks the tile geometry at this height (and the Fermat variant)
     tune_report = e.autotune(LO) if args.autotune else "off"
@@ -205,6 +201,8 @@ def run_ours(args):
     # results of the timed steps (checked against the fixture when it is present)
     out = d_out.cpu().numpy().view(np.uint64)
     res = dict(zip(mp.STATS_FIELDS, [int(x) for x in out]))
+    # whole-job statistics of [LO, LO + world SPAN): one all-gather of 8 words after timing
+    res_job = shard.gather_join(res, "range", device=dev)
 
     # e2e through the host API: outputs copied to host memory every step
     e2e_ms = []
@@ -286,7 +284,7 @@ def run_ours(args):
     peaks = e.probe_peaks()
     hbm, hbm_src = peaks_file()
 
-    fermat = run_fermat(e, world, rank) if not args.quick else None
+    fermat = run_fermat(e, world, rank, dev) if not args.quick else None
     serving = run_serving(e, args) if (rank == 0 and not args.quick and args.serve_requests) else None
 
     line = None
@@ -347,7 +345,8 @@ def run_ours(args):
             "serving": serving,
             "autotune": tune_report.strip().splitlines()[-3:] if tune_report != "off" else "off",
             "probes": peaks,
-            "results": res, "results_match_fixture": (res == ref_fixture) if (ref_fixture and rank == 0 and lo == LO) else None,
+            "results": res, "results_job": res_job if world > 1 else None,
+            "results_match_fixture": (res == ref_fixture) if (ref_fixture and rank == 0 and lo == LO) else None,
             "clocks": clocks,
         }
         if cpu:
@@ -360,7 +359,7 @@ def run_ours(args):
         print(json.dumps(line), flush=True)
 
 
-def run_fermat(e, world, rank):
+def run_fermat(e, world, rank, dev):
     """Config 4: every prime in [1e12 + r 4e9, 1e12 + (r+1) 4e9) from the GPU sieve, base-2
     Fermat quotients with the full statistics; device time of the quotient and reduction
     kernels (events on the handle's stream), and the host-API call end to end."""
@@ -371,6 +370,8 @@ def run_fermat(e, world, rank):
     r = e.wieferich_range(lo, hi)
     wall = time.perf_counter() - t0
     kms = e.last_kernel_ms()
+    from mathpub_b200 import shard
+    job = shard.gather_join(r, "wieferich", device=dev) if world > 1 else None
     fix = None
     try:
         with open(os.path.join(ROOT, "tests", "golden", "configs.json")) as f:
@@ -381,7 +382,8 @@ def run_fermat(e, world, rank):
     return {"workload": "base-2 Fermat quotients of every prime in [1e12, 1e12+4e9) (per rank), 3-limb Montgomery",
             "tests": r["tests"], "tests_per_s": r["tests"] / (kms / 1e3), "kernel_ms": kms,
             "e2e_tests_per_s": r["tests"] / wall, "e2e_ms": wall * 1e3, "near": r["near"], "flt": r["flt"],
-            "cks": r["cks"], "results_match_fixture": fix}
+            "cks": r["cks"], "results_match_fixture": fix,
+            "job": {k: job[k] for k in ("primes", "tests", "near", "flt", "cks", "ordered_hash", "nhits")} if job else None}
 
 
 def run_serving(e, args):
