@@ -102,20 +102,21 @@ class ClockSampler:
 
 
 def algorithmic_work(primes, lo, hi, tile_bits):
-    """Exact marks of the sieve (odd multiples m of each sieving prime q >= 97 with
-    max(lo, q^2) <= m < hi + tail) split at the tile size: marks by primes q <= tile_bits are
+    """Exact marks of the sieve: the multiples m = k q of each sieving prime q >= 97 with k
+    coprime to 30 (the wheel of 30; the presieve patterns mark the multiples of 3 and 5) and
+    max(lo, q^2) <= m < hi + tail, split at the tile size: marks by primes q <= tile_bits are
     shared-memory atomics, those above are bucket records (4 bytes written + 4 read)."""
     qi = primes[primes >= 97].astype(np.uint64)
     top = hi + (1 << 16)
     start = np.maximum(np.full(len(qi), lo, dtype=np.uint64), qi * qi)
-    # odd multiples of q in [start, top): multiples k q with k odd
-    def count_odd_mult(a, b, q):
-        # number of odd k with a <= k q < b
-        k0 = (a + q - np.uint64(1)) // q
-        k1 = (b + q - np.uint64(1)) // q          # first k with k q >= b
-        odd_below = lambda k: k // np.uint64(2)   # odd numbers < k
-        return (odd_below(k1) - odd_below(k0)).astype(np.float64)
-    m = count_odd_mult(start, np.full(len(qi), top, dtype=np.uint64), qi)
+    below = np.array([sum(1 for r in (1, 7, 11, 13, 17, 19, 23, 29) if r < x) for x in range(30)], dtype=np.uint64)
+
+    def coprime_below(k):                          # k' < k with gcd(k', 30) = 1
+        return np.uint64(8) * (k // np.uint64(30)) + below[(k % np.uint64(30)).astype(np.int64)]
+
+    k0 = (start + qi - np.uint64(1)) // qi         # first k with k q >= start
+    k1 = np.maximum((np.uint64(top) + qi - np.uint64(1)) // qi, k0)
+    m = (coprime_below(k1) - coprime_below(k0)).astype(np.float64)
     small = qi <= np.uint64(tile_bits)
     return float(m[small].sum()), float(m[~small].sum())
 

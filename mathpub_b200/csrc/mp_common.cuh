@@ -73,6 +73,47 @@ __device__ __forceinline__ u64 mp_first_odd_multiple(u64 x0, u32 q, u32 r, u64 c
     return j < cap ? j : cap;
 }
 
+// Wheel of 30 over the odd-only map.  The odd multiples q k of a sieving prime q lie q bits
+// apart.  Those with 3 | k or 5 | k are multiples of 3 or 5, which the presieve patterns mark
+// in every tile, so a prime q >= 7 marks only the q k with k coprime to 30: 8 of every 15.
+// After k = R[w] (mod 30), R = 1, 7, 11, 13, 17, 19, 23, 29, the next such multiple lies
+// D[w] q bits on, D = 3, 2, 1, 2, 1, 2, 3, 1 (the 2-bit fields of MP_W30_STEP); one turn of
+// the wheel is 15 q bits.
+#define MP_W30_STEP 0x799Bu
+#define MP_W30_STEP2 0x799B799Bu        // two copies, so rotations by 2 w keep the sequence
+// for odd k mod 30 = 2h + 1: the index w of the first R[w] >= 2h + 1 (3-bit fields) and the
+// distance to it in q bits (2-bit fields)
+#define MP_W30_IDX 0x1ffdac8d2248ull
+#define MP_W30_ADV 0x6104118u
+
+// j: bit of an odd multiple q k of the sieving prime q >= 7 (bit j <-> x0 + 2 j), xm = x0 mod
+// 30.  Returns the bit of the first multiple q k' >= q k with k' coprime to 30 and sets *w to
+// the index of k' mod 30 in R.  k mod 30 = (x0 + 2 j) q^-1 mod 30, and q^-1 = q^3 mod 30
+// because every unit mod 30 has an order dividing 4.
+__device__ __forceinline__ u64 mp_w30_first(u32 j, u32 xm, u32 q, u32 *w)
+{
+    const u32 c = q % 30u;
+    const u32 inv = (c * c % 30u) * c % 30u;
+    const u32 t = (xm + 2u * (j % 15u)) % 30u;
+    const u32 h = (t * inv % 30u) >> 1;
+    *w = (u32)(MP_W30_IDX >> (3u * h)) & 7u;
+    return (u64)j + (u64)q * ((MP_W30_ADV >> (2u * h)) & 3u);
+}
+
+// the step fields from residue index w on: the next step is s & 3, then s = rotr(s, 2)
+__device__ __forceinline__ u32 mp_w30_steps(u32 w)
+{
+    return __funnelshift_r(MP_W30_STEP2, MP_W30_STEP2, 2u * w);
+}
+
+// sum of the first n (<= 8) step fields of s: the distance in q bits from the residue s starts
+// at to the n-th one after it
+__device__ __forceinline__ u32 mp_w30_span(u32 s, u32 n)
+{
+    const u32 x = s & ((1u << (2u * n)) - 1u);
+    return __popc(x & 0x55555555u) + 2u * __popc(x & 0xAAAAAAAAu);
+}
+
 // ---------------------------------------------------------------------------------------
 // handle
 // ---------------------------------------------------------------------------------------
@@ -162,7 +203,7 @@ struct mp_handle {
 
     // scratch
     DevBuf tilesum, blockacc, rec, reccnt, queue, errflag, scratch_bitmap, bpsw_n, bpsw_bits,
-        ferm_p, ferm_q, ferm_part, stats_out, small_out, scat_bounds;
+        ferm_p, ferm_q, ferm_part, stats_out, small_out, scat_bounds, tstate;
     u64 scat_key[3] = {~0ull, ~0ull, ~0ull};   // (first, end, blocks) the bounds were built for
     std::vector<u32> scat_host;
     u32 scat_nblk = 0;

@@ -60,7 +60,7 @@ struct TileArgs {
     u32 t0, nt;                          // tiles [t0, t0 + nt) of this launch
     const u32 *q;
     const u64 *magic;
-    u32 iw0, iw1, it1;                   // warp tier [iw0, iw1), thread tier [iw1, it1)
+    u32 iw0, iw1, itd, it1;              // warp tier [iw0, iw1), thread tier [iw1, itd) dense, [itd, it1) sparse
     const u32 *pat[MP_NPAT];
     u32 period[MP_NPAT];
     const u32 *rec;                      // bucket records of tiles [t0, t0 + nt) (nullable)
@@ -71,8 +71,13 @@ struct TileArgs {
     const u64 *emit_off;                 // emit mode: per-tile offset of its first prime
     u64 *emit64;
     u32 *emit32;
-    u32 *queue;
+    u32 *tstate;                         // per CTA: next multiple of each sparse thread-tier prime
 };
+
+// state of a sparse thread-tier prime between the tiles of a CTA's run: (next bit relative to
+// the next tile) << 3 | wheel index, or W30_NOSTATE (set it up from x0 again)
+#define W30_NOSTATE 0xffffffffu
+#define W30_FAR (1u << 28)
 
 // ---------------------------------------------------------------------------------------
 // ordered combine of tile / thread summaries
@@ -198,7 +203,6 @@ __global__ void __launch_bounds__(1024) tile_kernel(TileArgs a)
     constexpr u32 TW = T / 32;
     constexpr u32 NB = T + HALO_BITS;          // bits held in shared memory
     extern __shared__ __align__(16) u32 sm[];  // TW + HALO_WORDS words
-    __shared__ u32 s_tile;
     __shared__ u32 s_off[MP_NPAT];
     __shared__ Part s_part[32];
     __shared__ u32 s_cnt[32];
@@ -206,11 +210,15 @@ __global__ void __launch_bounds__(1024) tile_kernel(TileArgs a)
     const u32 tid = threadIdx.x, nth = blockDim.x, lane = tid & 31, warp = tid >> 5, nwarps = nth >> 5;
     const u64 base = a.g.base, limit = a.g.limit, nbx = a.g.nbx;
 
-    for (;;) {
-        if (tid == 0) s_tile = atomicAdd(a.queue, 1u);
-        __syncthreads();
-        const u32 rel = s_tile;
+    // CTA b sieves the contiguous run of tiles [b per, (b + 1) per) of the launch, so that the
+    // sparse thread-tier primes carry their next multiple from one tile to the next
+    const u32 per = (a.nt + gridDim.x - 1) / gridDim.x;
+    u32 *const tst = a.tstate + (u64)blockIdx.x * (a.it1 - a.itd);
+    for (u32 run = 0; run < per; run++) {
+        const u32 rel = blockIdx.x * per + run;
         if (rel >= a.nt) break;
+        const bool fresh = run == 0;                              // no carried state yet
+        const bool keep = run + 1 < per && rel + 1 < a.nt;        // the next tile follows here
         const u32 t = a.t0 + rel;
         const u64 G = (u64)t << TLOG;           // first bit of the tile
         const u64 x0 = base + 2 * G + 1;        // the odd number of that bit
@@ -233,19 +241,76 @@ __global__ void __launch_bounds__(1024) tile_kernel(TileArgs a)
             if (x0 == 1) atomicOr(&sm[0], 1u);
         }
 
-        // 2. warp tier: one warp per prime, lanes on consecutive multiples
+        // multiples q k with k coprime to 30 only (wheel of 30; the patterns hold 3 and 5)
+        const u32 xm = (u32)(x0 % 30u);
+        // 2. warp tier: one warp per prime; lane l walks residue (l & 7) of the wheel in turn
+        //    (l >> 3), four turns (60 q bits) per step
         for (u32 k = a.iw0 + warp; k < a.iw1; k += nwarps) {
             const u32 q = __ldg(a.q + k);
             const u32 r = mp_mod_barrett(x0, q, __ldg(a.magic + k));
-            const u32 j0 = (u32)mp_first_odd_multiple(x0, q, r, NB);
-            for (u32 j = j0 + lane * q; j < NB; j += 32 * q) atomicOr(&sm[j >> 5], 1u << (j & 31));
+            const u64 j64 = mp_first_odd_multiple(x0, q, r, NB);
+            if (j64 >= NB) continue;
+            u32 w;
+            const u32 jw = (u32)mp_w30_first((u32)j64, xm, q, &w);
+            const u32 j0 = jw + q * (mp_w30_span(mp_w30_steps(w), lane & 7) + 15u * (lane >> 3));
+            for (u32 j = j0; j < NB; j += 60u * q) atomicOr(&sm[j >> 5], 1u << (j & 31));
         }
-        // 3. thread tier: one thread per prime
-        for (u32 k = a.iw1 + tid; k < a.it1; k += nth) {
+        // 3. thread tier, one thread per prime.  Dense primes (q < T / 32) have several
+        //    multiples per residue of the wheel in a tile: set up from x0 in every tile and
+        //    walked as 8 progressions of stride 15 q.
+        for (u32 k = a.iw1 + tid; k < a.itd; k += nth) {
             const u32 q = __ldg(a.q + k);
             const u32 r = mp_mod_barrett(x0, q, __ldg(a.magic + k));
-            for (u32 j = (u32)mp_first_odd_multiple(x0, q, r, NB); j < NB; j += q)
-                atomicOr(&sm[j >> 5], 1u << (j & 31));
+            const u64 j64 = mp_first_odd_multiple(x0, q, r, NB);
+            if (j64 >= NB) continue;
+            u32 w;
+            u32 j = (u32)mp_w30_first((u32)j64, xm, q, &w);
+            u32 s = mp_w30_steps(w);
+            const u32 turn = 15u * q;
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+                for (u32 jj = j; jj < NB; jj += turn) atomicOr(&sm[jj >> 5], 1u << (jj & 31));
+                j += q * (s & 3u);
+                s >>= 2;
+            }
+        }
+        //    Sparse primes (T / 32 <= q <= T) have a few multiples per tile: one walk through
+        //    the residues, with the next multiple carried to the CTA's next tile, so that the
+        //    modular set-up runs once per run of tiles.  Four primes per thread are loaded
+        //    ahead.
+        for (u32 k = a.itd + tid; k < a.it1; k += 4 * nth) {
+            u32 qv[4], sv[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const u32 kk = k + u * nth;
+                qv[u] = kk < a.it1 ? __ldg(a.q + kk) : 0u;
+                sv[u] = (kk < a.it1 && !fresh) ? tst[kk - a.itd] : W30_NOSTATE;
+            }
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const u32 q = qv[u];
+                if (!q) continue;
+                const u32 kk = k + u * nth;
+                u32 j, w;
+                if (sv[u] == W30_NOSTATE) {
+                    const u32 r = mp_mod_barrett(x0, q, __ldg(a.magic + kk));
+                    const u64 j64 = mp_first_odd_multiple(x0, q, r, W30_FAR);
+                    if (j64 >= W30_FAR) {                      // q^2 far beyond this tile
+                        if (keep) tst[kk - a.itd] = W30_NOSTATE;
+                        continue;
+                    }
+                    j = (u32)mp_w30_first((u32)j64, xm, q, &w);
+                } else {
+                    j = sv[u] >> 3;
+                    w = sv[u] & 7u;
+                }
+                u32 s = mp_w30_steps(w), n = 0;
+                for (; j < T; j += q * (s & 3u), s = __funnelshift_r(s, s, 2), n++)
+                    atomicOr(&sm[j >> 5], 1u << (j & 31));
+                if (keep) tst[kk - a.itd] = ((j - T) << 3) | ((w + n) & 7u);
+                for (; j < NB; j += q * (s & 3u), s = __funnelshift_r(s, s, 2))     // halo bits
+                    atomicOr(&sm[j >> 5], 1u << (j & 31));
+            }
         }
         // 4. large primes: bucket records of this tile
         if (a.rec) {
@@ -468,11 +533,12 @@ struct ScatterArgs {
 
 // every hit j of prime q in the wave (plus the first HALO_BITS bits after it): record
 // (tile, offset) for its own tile, and (tile - 1, offset + 2^TLOG) when it lies in the first
-// HALO_BITS bits of a tile, because the previous tile sieves those bits as its halo
-// The hits of a prime in the wave are j0 + m q.  They are walked four at a time: the four
-// slot atomics are issued before the four record stores, so several atomics are in flight per
-// thread.  Lanes walk in lock step: lanes of a warp that hit the same tile take neighbouring
-// slots, which keeps their record stores together.
+// HALO_BITS bits of a tile, because the previous tile sieves those bits as its halo.
+// The hits are the multiples q k with k coprime to 30 (the wheel of 30): 8 progressions of
+// stride 15 q, walked together so that eight slot atomics are in flight per thread; in
+// pass 1 the eight slot atomics are issued before the eight record stores.  Lanes walk in
+// lock step: lanes of a warp that hit the same tile take neighbouring slots, which keeps
+// their record stores together.
 template <int PASS>
 __device__ __forceinline__ void scatter_halo(const ScatterArgs &a, u32 tl, u32 off, u32 *scnt, const u32 *sbase)
 {
@@ -488,48 +554,51 @@ __device__ __forceinline__ void scatter_halo(const ScatterArgs &a, u32 tl, u32 o
 }
 
 template <int PASS>
-__device__ __forceinline__ void scatter_prime(const ScatterArgs &a, u32 k, u64 x0, u32 span, u32 *scnt, const u32 *sbase)
+__device__ __forceinline__ void scatter_prime(const ScatterArgs &a, u32 k, u64 x0, u32 xm, u32 span, u32 *scnt,
+                                              const u32 *sbase)
 {
     const u32 q = __ldg(a.q + k);
     const u32 r = mp_mod_barrett(x0, q, __ldg(a.magic + k));
     const u64 j64 = mp_first_odd_multiple(x0, q, r, span);
     if (j64 >= span) return;
-    const u32 j0 = (u32)j64;                           // bit relative to the wave (tile aligned)
-    const u32 H = (span - 1 - j0) / q + 1;             // hits in [j0, span)
-    const u32 tlog = a.tlog, tmask = (1u << tlog) - 1, wt = a.wt;
-    u32 m = 0, j = j0;
-    for (; m + 4 <= H; m += 4, j += 4 * q) {
-        u32 jj[4], tl[4], sl[4];
+    u32 w;
+    u64 j = mp_w30_first((u32)j64, xm, q, &w);         // bits relative to the wave (tile aligned)
+    u32 s = mp_w30_steps(w);
+    // span < 2^31: a stride of 2^31 or more leaves one hit per progression at most, so the
+    // stride is clamped there and the positions stay below 2^32
+    const u64 turn64 = 15ull * q;
+    const u32 turn = turn64 >= (1ull << 31) ? (1u << 31) : (u32)turn64;
+    u32 jj[8];
 #pragma unroll
-        for (int u = 0; u < 4; u++) { jj[u] = j + u * q; tl[u] = jj[u] >> tlog; }
+    for (int i = 0; i < 8; i++) {                      // ascending starts, all below j + 15 q
+        jj[i] = j < span ? (u32)j : span;
+        j += (u64)q * (s & 3u);
+        s >>= 2;
+    }
+    const u32 tlog = a.tlog, tmask = (1u << tlog) - 1, wt = a.wt;
+    while (jj[0] < span) {
+        u32 tl[8], sl[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) tl[i] = jj[i] < span ? jj[i] >> tlog : 0xffffffffu;
         if (PASS == 0) {
 #pragma unroll
-            for (int u = 0; u < 4; u++) if (tl[u] < wt) atomicAdd(&scnt[tl[u]], 1u);
+            for (int i = 0; i < 8; i++) if (tl[i] < wt) atomicAdd(&scnt[tl[i]], 1u);
         } else {
 #pragma unroll
-            for (int u = 0; u < 4; u++) sl[u] = tl[u] < wt ? sbase[tl[u]] + atomicAdd(&scnt[tl[u]], 1u) : 0;
+            for (int i = 0; i < 8; i++) sl[i] = tl[i] < wt ? sbase[tl[i]] + atomicAdd(&scnt[tl[i]], 1u) : 0;
 #pragma unroll
-            for (int u = 0; u < 4; u++) {
-                if (tl[u] < wt) {
-                    if (sl[u] < a.cap) a.rec[(u64)tl[u] * a.cap + sl[u]] = jj[u] & tmask;
+            for (int i = 0; i < 8; i++) {
+                if (tl[i] < wt) {
+                    if (sl[i] < a.cap) a.rec[(u64)tl[i] * a.cap + sl[i]] = jj[i] & tmask;
                     else atomicOr(a.err, 2u);
                 }
             }
         }
 #pragma unroll
-        for (int u = 0; u < 4; u++) scatter_halo<PASS>(a, tl[u], jj[u] & tmask, scnt, sbase);
-    }
-    for (; m < H; m++, j += q) {
-        const u32 tl = j >> tlog, off = j & tmask;
-        if (tl < wt) {
-            if (PASS == 0) atomicAdd(&scnt[tl], 1u);
-            else {
-                const u32 slot = sbase[tl] + atomicAdd(&scnt[tl], 1u);
-                if (slot < a.cap) a.rec[(u64)tl * a.cap + slot] = off;
-                else atomicOr(a.err, 2u);
-            }
+        for (int i = 0; i < 8; i++) {
+            if (tl[i] != 0xffffffffu) scatter_halo<PASS>(a, tl[i], jj[i] & tmask, scnt, sbase);
+            jj[i] = jj[i] < span ? jj[i] + turn : span;
         }
-        scatter_halo<PASS>(a, tl, off, scnt, sbase);
     }
 }
 
@@ -548,7 +617,8 @@ __global__ void __launch_bounds__(512) scatter_kernel(ScatterArgs a)
     const u64 x0 = a.base + 2 * wstart + 1;
     const u32 k0 = __ldg(a.bounds + blockIdx.x), k1 = __ldg(a.bounds + blockIdx.x + 1);
     const u32 span = (u32)(wend_halo - wstart);        // < 2^31 (checked by the planner)
-    for (u32 k = k0 + tid; k < k1; k += nth) scatter_prime<0>(a, k, x0, span, scnt, sbase);
+    const u32 xm = (u32)(x0 % 30u);
+    for (u32 k = k0 + tid; k < k1; k += nth) scatter_prime<0>(a, k, x0, xm, span, scnt, sbase);
     __syncthreads();
     for (u32 i = tid; i < a.wt; i += nth) {
         const u32 c = scnt[i];
@@ -556,7 +626,7 @@ __global__ void __launch_bounds__(512) scatter_kernel(ScatterArgs a)
         scnt[i] = 0;
     }
     __syncthreads();
-    for (u32 k = k0 + tid; k < k1; k += nth) scatter_prime<1>(a, k, x0, span, scnt, sbase);
+    for (u32 k = k0 + tid; k < k1; k += nth) scatter_prime<1>(a, k, x0, xm, span, scnt, sbase);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -846,7 +916,7 @@ int mp_patterns_ensure(mp_handle *h)
 // host driver
 // ---------------------------------------------------------------------------------------
 
-struct Tiers { u32 iw0, iw1, it1, iend; };
+struct Tiers { u32 iw0, iw1, itd, it1, iend; };
 
 static Tiers tiers_for(const PrimeTable &tb, u32 tlog, u64 top)
 {
@@ -856,6 +926,7 @@ static Tiers tiers_for(const PrimeTable &tb, u32 tlog, u64 top)
     r.iw0 = (u32)std::min<u64>(tb.count_le(PAT_MAXQ), r.iend);
     r.iw1 = (u32)std::min<u64>(tb.count_le(QWARP - 1), r.iend);
     r.it1 = (u32)std::min<u64>(tb.count_le(1ull << tlog), r.iend);
+    r.itd = std::max(r.iw1, (u32)std::min<u64>(tb.count_le((1ull << tlog) / 32 - 1), r.it1));
     return r;
 }
 
@@ -901,12 +972,13 @@ static int tile_ctas_per_sm(u32 tlog, int nth)
 }
 
 // expected bucket records per tile for the large primes (Mertens' theorem: the sum of 1/q
-// over primes in (a, b] is about ln(ln b / ln a)), with a margin
+// over primes in (a, b] is about ln(ln b / ln a); the wheel of 30 keeps 8 of every 15 odd
+// multiples), with a margin
 static u32 bucket_cap(u32 tlog, u64 qmax)
 {
     const double T = (double)(1u << tlog) + HALO_BITS;
     const double a = (double)(1u << tlog);
-    double s = qmax > (u64)a ? log(log((double)qmax) / log(a)) : 0.0;
+    double s = qmax > (u64)a ? log(log((double)qmax) / log(a)) * (8.0 / 15.0) : 0.0;
     double e = T * s * 1.06 + 8.0 * sqrt(T * s + 1.0) + 4096.0;
     if (e > 4.0e9) e = 4.0e9;
     return ((u32)e + 3) & ~3u;
@@ -959,7 +1031,7 @@ static void fill_tile_args(mp_handle *h, const PrimeTable &tb, const SievePlan &
     a.g = P.g;
     a.q = tb.q.as<u32>();
     a.magic = tb.magic.as<u64>();
-    a.iw0 = P.ti.iw0; a.iw1 = P.ti.iw1; a.it1 = P.ti.it1;
+    a.iw0 = P.ti.iw0; a.iw1 = P.ti.iw1; a.itd = P.ti.itd; a.it1 = P.ti.it1;
     for (int p = 0; p < MP_NPAT; p++) { a.pat[p] = h->pat.d_words[p]; a.period[p] = h->pat.period[p]; }
 }
 
@@ -1015,14 +1087,18 @@ static int scatter_bounds(mp_handle *h, const PrimeTable &tb, u32 i0, u32 i1, cu
     return MP_OK;
 }
 
-// mode: 0 batched (waves of persistent tile launches), 1 plain (one launch per tile)
+// mode: 0 batched (waves of tile launches, each CTA a contiguous run of tiles), 1 plain (one
+// launch per tile)
 static int run_tiles(mp_handle *h, const PrimeTable &tb, const SievePlan &P, TileArgs a, int mode, int emit,
                      cudaStream_t st)
 {
     const int nth = P.nth;
     const u32 nlaunch = mode == 1 ? P.g.ntiles : P.nwaves;
-    MP_CUDA(h, h->queue.ensure((size_t)nlaunch * 4 + 64));
-    MP_CUDA(h, cudaMemsetAsync(h->queue.p, 0, (size_t)nlaunch * 4 + 64, st));
+    const int grid_pers = h->sm_count * tile_ctas_per_sm(P.g.tlog, nth);
+    // carried state of the sparse thread-tier primes: one slot per prime per CTA (written and
+    // read by the tile kernel only; nothing needs clearing)
+    MP_CUDA(h, h->tstate.ensure((size_t)grid_pers * (P.ti.it1 - P.ti.itd) * 4 + 64));
+    a.tstate = h->tstate.as<u32>();
     u32 *errp = h->errflag.as<u32>();
     if (P.large) {
         const u32 wt = mode == 1 ? 1 : P.wt;
@@ -1030,7 +1106,6 @@ static int run_tiles(mp_handle *h, const PrimeTable &tb, const SievePlan &P, Til
         MP_CUDA(h, h->reccnt.ensure((size_t)wt * 4 * 2));
     }
     if (P.large) MP_TRY(scatter_bounds(h, tb, P.ti.it1, P.ti.iend, st));
-    const int grid_pers = h->sm_count * tile_ctas_per_sm(P.g.tlog, nth);
     for (u32 L = 0; L < nlaunch; L++) {
         const u32 t0 = mode == 1 ? L : L * P.wt;
         const u32 nt = mode == 1 ? 1 : std::min(P.wt, P.g.ntiles - t0);
@@ -1050,7 +1125,6 @@ static int run_tiles(mp_handle *h, const PrimeTable &tb, const SievePlan &P, Til
             a.rec = s.rec; a.reccnt = s.cnt; a.reccap = P.cap;
         }
         a.t0 = t0; a.nt = nt;
-        a.queue = h->queue.as<u32>() + L;
         const int grid = mode == 1 ? 1 : (int)std::min<u64>((u64)grid_pers, nt);
         ProfScope ps(h, PROF_TILE, st);
         MP_CUDA(h, launch_tile_any(a, grid, nth, emit, st));
