@@ -778,10 +778,27 @@ __global__ void __launch_bounds__(512) fold_kernel(FoldArgs a)
 }
 
 // ---------------------------------------------------------------------------------------
-// FNV-1a-64 per hash segment of the bitmap (one thread per segment: the hash is a chain)
+// FNV-1a-64 per hash segment of the bitmap.  The hash is a serial chain over the segment's
+// bytes, so each thread hashes one segment; one warp per CTA spreads the segments over every
+// SM.  Each thread keeps HASH_AHEAD 16-byte loads (256 bytes) in flight ahead of its chain,
+// which otherwise waits on every load.
 // ---------------------------------------------------------------------------------------
 
-__global__ void hash_kernel(const u32 *__restrict__ bm, u64 nbits, u64 seg_bits, u64 nseg, u64 *out)
+#define HASH_AHEAD 16
+
+__device__ __forceinline__ void fnv_word(u64 &h, u32 w)
+{
+#pragma unroll
+    for (int j = 0; j < 4; j++) { h ^= (w >> (8 * j)) & 0xffu; h *= MP_FNV_PRIME; }
+}
+
+__device__ __forceinline__ void fnv_16(u64 &h, const uint4 v)
+{
+    fnv_word(h, v.x); fnv_word(h, v.y); fnv_word(h, v.z); fnv_word(h, v.w);
+}
+
+__global__ void __launch_bounds__(32) hash_kernel(const u32 *__restrict__ bm, u64 nbits, u64 seg_bits, u64 nseg,
+                                                  u64 *out)
 {
     const u64 s = (u64)blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= nseg) return;
@@ -791,16 +808,31 @@ __global__ void hash_kernel(const u32 *__restrict__ bm, u64 nbits, u64 seg_bits,
     const u8 *p = (const u8 *)bm + (b0 >> 3);       // seg_bits is a multiple of 8
     u64 h = MP_FNV_OFFSET;
     u64 k = 0;
-    // 16-byte loads where aligned
-    while (k < nbytes && (((uintptr_t)(p + k)) & 15)) { h ^= p[k]; h *= MP_FNV_PRIME; k++; }
-    for (; k + 16 <= nbytes; k += 16) {
-        const uint4 v = __ldg((const uint4 *)(p + k));
-        const u32 w[4] = {v.x, v.y, v.z, v.w};
+    // bytes up to a 16-byte boundary (all but the last byte of the segment are whole)
+    for (; k + 1 < nbytes && (((uintptr_t)(p + k)) & 15); k++) { h ^= p[k]; h *= MP_FNV_PRIME; }
+    // whole blocks of HASH_AHEAD 16-byte words: the loads of block b + 1 are issued while
+    // block b is hashed
+    const u64 nblk = nbytes > k + 1 ? (nbytes - k - 1) / (16 * HASH_AHEAD) : 0;
+    if (nblk) {
+        const uint4 *v = (const uint4 *)(p + k);
+        uint4 buf[HASH_AHEAD];
 #pragma unroll
-        for (int i = 0; i < 4; i++)
+        for (int i = 0; i < HASH_AHEAD; i++) buf[i] = __ldg(v + i);
+        for (u64 b = 0; b < nblk; b++) {
+            const uint4 *nx = v + (b + 1) * HASH_AHEAD;
+            const bool more = b + 1 < nblk;
 #pragma unroll
-            for (int j = 0; j < 4; j++) { h ^= (w[i] >> (8 * j)) & 0xff; h *= MP_FNV_PRIME; }
+            for (int i = 0; i < HASH_AHEAD; i++) {
+                const uint4 x = buf[i];
+                if (more) buf[i] = __ldg(nx + i);
+                fnv_16(h, x);
+            }
+        }
+        k += nblk * 16 * HASH_AHEAD;
     }
+    // the rest in 16-byte words while one byte more remains, then bytes; the last byte keeps
+    // only the bits of the segment
+    for (; k + 16 < nbytes; k += 16) fnv_16(h, __ldg((const uint4 *)(p + k)));
     for (; k < nbytes; k++) {
         u8 c = p[k];
         const u64 rem = len - 8 * k;
@@ -1305,7 +1337,7 @@ int mp_sieve_run(mp_handle *h, u64 lo, u64 hi, const mp_sieve_opts *o, mp_range_
         const u64 sb = 1ull << (hash_log2 - 1);
         const u64 ns = (P.g.limit + sb - 1) / sb;
         ProfScope ps(h, PROF_HASH, st);
-        hash_kernel<<<(unsigned)((ns + 127) / 128), 128, 0, st>>>(bm, P.g.limit, sb, ns, d_hash);
+        hash_kernel<<<(unsigned)((ns + 31) / 32), 32, 0, st>>>(bm, P.g.limit, sb, ns, d_hash);
         MP_CUDA(h, cudaGetLastError());
     }
     return MP_OK;
