@@ -356,6 +356,7 @@ __global__ void __launch_bounds__(1024) tile_kernel(TileArgs a)
             u32 first = NONE32, last = NONE32, lastin = NONE32, bg = 0, bs = NONE32, carry = NONE32;
             const u64 lim_rel = limit > G ? limit - G : 0;         // bits of the tile below limit
             const u64 nbx_rel = nbx > G ? nbx - G : 0;
+            u32 thr = 0;                                             // the warp's widest gap so far
             for (u32 r = 0; r < wpw; r += 128) {
                 const u32 w = wbase + r + 4 * lane;
                 const uint4 v = *(const uint4 *)&sm[w];
@@ -392,16 +393,39 @@ __global__ void __launch_bounds__(1024) tile_kernel(TileArgs a)
                         }
                     }
                     if (pin) lastin = b0 + 32 * k + 31 - __clz(pin);
-                    u32 y = pk;
-                    while (y) {                              // gaps inside the lane's 128 bits
-                        const u32 pos = b0 + 32 * k + __ffs(y) - 1;
-                        y &= y - 1;
-                        if (ll == NONE32) lf = pos;
-                        else if ((u64)ll < lim_rel) {
-                            const u32 g = pos - ll;
-                            if (g > bg || (g == bg && ll < bs)) { bg = g; bs = ll; }
+                }
+                // gaps inside the lane's 128 bits.  While the warp's widest gap is below 32
+                // bits every prime is walked.  From 32 bits on, a gap inside one 32-bit word
+                // can neither beat nor tie it, so only the gaps from the last prime of a word
+                // to the first prime of a later one are taken (thr is the same in every lane).
+                if (thr < 32) {
+#pragma unroll
+                    for (int k = 0; k < 4; k++) {
+                        u32 y = p[k];
+                        while (y) {
+                            const u32 pos = b0 + 32 * k + __ffs(y) - 1;
+                            y &= y - 1;
+                            if (ll == NONE32) lf = pos;
+                            else if ((u64)ll < lim_rel) {
+                                const u32 g = pos - ll;
+                                if (g > bg || (g == bg && ll < bs)) { bg = g; bs = ll; }
+                            }
+                            ll = pos;
                         }
-                        ll = pos;
+                    }
+                } else {
+#pragma unroll
+                    for (int k = 0; k < 4; k++) {
+                        const u32 pk = p[k];
+                        if (pk) {
+                            const u32 f = b0 + 32 * k + __ffs(pk) - 1;
+                            if (ll == NONE32) lf = f;
+                            else if ((u64)ll < lim_rel) {
+                                const u32 g = f - ll;
+                                if (g > bg || (g == bg && ll < bs)) { bg = g; bs = ll; }
+                            }
+                            ll = b0 + 32 * k + 31 - __clz(pk);
+                        }
                     }
                 }
                 // last prime before this lane's first: inclusive max-scan of (last + 1)
@@ -420,6 +444,9 @@ __global__ void __launch_bounds__(1024) tile_kernel(TileArgs a)
                 }
                 const u32 rowlast = __shfl_sync(0xffffffffu, sc, 31);
                 if (rowlast) carry = rowlast - 1;
+                thr = bg;
+#pragma unroll
+                for (int d = 16; d >= 1; d >>= 1) thr = max(thr, __shfl_xor_sync(0xffffffffu, thr, d));
                 if (first == NONE32 && lf != NONE32) first = lf;
                 if (ll != NONE32) last = ll;
             }
