@@ -161,7 +161,6 @@ struct PrimeTable {
     DevBuf magic;                    // u64[n] floor((2^64-1)/q)
     std::vector<u32> host;
     std::vector<double> inv_prefix;  // inv_prefix[i] = sum of 1/q over the first i primes
-    std::vector<u32> work_bounds;    // prime indices cutting the table into runs of equal sum 1/q
     u64 count_le(u64 x) const;       // number of table primes <= x
 };
 

@@ -558,102 +558,177 @@ struct ScatterArgs {
     u32 *err;
 };
 
-// every hit j of prime q in the wave (plus the first HALO_BITS bits after it): record
-// (tile, offset) for its own tile, and (tile - 1, offset + 2^TLOG) when it lies in the first
-// HALO_BITS bits of a tile, because the previous tile sieves those bits as its halo.
+// Every hit j of a large prime q in the wave (plus the first HALO_BITS bits after it) is a
+// record (tile, offset) of its own tile, and also (tile - 1, offset + 2^TLOG) when it lies in
+// the first HALO_BITS bits of a tile, because the previous tile sieves those bits as its halo.
 // The hits are the multiples q k with k coprime to 30 (the wheel of 30): 8 progressions of
-// stride 15 q, walked together so that eight slot atomics are in flight per thread; in
-// pass 1 the eight slot atomics are issued before the eight record stores.  Lanes walk in
-// lock step: lanes of a warp that hit the same tile take neighbouring slots, which keeps
-// their record stores together.
-template <int PASS>
-__device__ __forceinline__ void scatter_halo(const ScatterArgs &a, u32 tl, u32 off, u32 *scnt, const u32 *sbase)
-{
-    // a hit in the first HALO_BITS bits of tile tl is also a record of tile tl - 1 (its halo)
-    if (off < HALO_BITS && tl >= 1 && tl - 1 < a.wt) {
-        if (PASS == 0) atomicAdd(&scnt[tl - 1], 1u);
-        else {
-            const u32 slot = sbase[tl - 1] + atomicAdd(&scnt[tl - 1], 1u);
-            if (slot < a.cap) a.rec[(u64)(tl - 1) * a.cap + slot] = off + (1u << a.tlog);
-            else atomicOr(a.err, 2u);
-        }
-    }
-}
+// stride 15 q.
+//
+// One pass, staged in shared memory: each persistent CTA owns a run of primes of equal sum
+// of 1/q (equal expected hits); every thread walks one prime at a time, one turn of the wheel
+// (8 hits) per round, and appends the records to the CTA's stage with one shared atomic per
+// warp.  When the stage is nearly full the CTA sorts it by tile (counting sort), reserves one
+// run per tile in the bucket with one global atomic, and writes the runs out, so that the
+// record stores of a warp are coalesced.  Halo copies (one hit in 1024) go to the bucket
+// directly.
 
-template <int PASS>
-__device__ __forceinline__ void scatter_prime(const ScatterArgs &a, u32 k, u64 x0, u32 xm, u32 span, u32 *scnt,
-                                              const u32 *sbase)
+#define SC_THREADS 512
+#define SC_STAGE 12288                    // staged records per CTA; two CTAs per SM
+#define SC_OFF_BITS 21                    // staged record: tile << 21 | offset (offset < 2^21)
+
+// set up prime k: the 8 progression starts (ascending, below j + 15 q) relative to the wave;
+// returns false when the prime has no hit in the wave
+__device__ __forceinline__ bool scatter_setup(const ScatterArgs &a, u32 k, u64 x0, u32 xm, u32 span, u32 *jj,
+                                              u32 &turn)
 {
     const u32 q = __ldg(a.q + k);
     const u32 r = mp_mod_barrett(x0, q, __ldg(a.magic + k));
     const u64 j64 = mp_first_odd_multiple(x0, q, r, span);
-    if (j64 >= span) return;
+    if (j64 >= span) return false;
     u32 w;
-    u64 j = mp_w30_first((u32)j64, xm, q, &w);         // bits relative to the wave (tile aligned)
+    u64 j = mp_w30_first((u32)j64, xm, q, &w);
     u32 s = mp_w30_steps(w);
     // span < 2^31: a stride of 2^31 or more leaves one hit per progression at most, so the
     // stride is clamped there and the positions stay below 2^32
     const u64 turn64 = 15ull * q;
-    const u32 turn = turn64 >= (1ull << 31) ? (1u << 31) : (u32)turn64;
-    u32 jj[8];
+    turn = turn64 >= (1ull << 31) ? (1u << 31) : (u32)turn64;
 #pragma unroll
-    for (int i = 0; i < 8; i++) {                      // ascending starts, all below j + 15 q
+    for (int i = 0; i < 8; i++) {
         jj[i] = j < span ? (u32)j : span;
         j += (u64)q * (s & 3u);
         s >>= 2;
     }
-    const u32 tlog = a.tlog, tmask = (1u << tlog) - 1, wt = a.wt;
-    while (jj[0] < span) {
-        u32 tl[8], sl[8];
-#pragma unroll
-        for (int i = 0; i < 8; i++) tl[i] = jj[i] < span ? jj[i] >> tlog : 0xffffffffu;
-        if (PASS == 0) {
-#pragma unroll
-            for (int i = 0; i < 8; i++) if (tl[i] < wt) atomicAdd(&scnt[tl[i]], 1u);
-        } else {
-#pragma unroll
-            for (int i = 0; i < 8; i++) sl[i] = tl[i] < wt ? sbase[tl[i]] + atomicAdd(&scnt[tl[i]], 1u) : 0;
-#pragma unroll
-            for (int i = 0; i < 8; i++) {
-                if (tl[i] < wt) {
-                    if (sl[i] < a.cap) a.rec[(u64)tl[i] * a.cap + sl[i]] = jj[i] & tmask;
-                    else atomicOr(a.err, 2u);
-                }
-            }
-        }
-#pragma unroll
-        for (int i = 0; i < 8; i++) {
-            if (tl[i] != 0xffffffffu) scatter_halo<PASS>(a, tl[i], jj[i] & tmask, scnt, sbase);
-            jj[i] = jj[i] < span ? jj[i] + turn : span;
-        }
-    }
+    return jj[0] < span;
 }
 
-__global__ void __launch_bounds__(512) scatter_kernel(ScatterArgs a)
+// sort the staged records by tile and write them to their buckets (all threads)
+__device__ __forceinline__ void scatter_flush(const ScatterArgs &a, u32 *stage, u32 *sorted, u32 *hist, u32 *gb,
+                                           u32 *s_fill, u32 *s_wsum)
 {
-    extern __shared__ u32 ssm[];             // scnt[wt], sbase[wt]
-    u32 *scnt = ssm, *sbase = ssm + a.wt;
-    const u32 tid = threadIdx.x, nth = blockDim.x;
-    for (u32 i = tid; i < a.wt; i += nth) scnt[i] = 0;
+    const u32 tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, wt = a.wt;
     __syncthreads();
-    const u64 wstart = (u64)a.t0 << a.tlog;
-    u64 wend = (u64)(a.t0 + a.wt) << a.tlog;
+    const u32 n = *s_fill;
+    // exclusive scan of the tile counts; thread t owns tiles [t per, (t + 1) per)
+    const u32 per = (wt + SC_THREADS - 1) / SC_THREADS;
+    const u32 t0 = tid * per;
+    u32 sum = 0;
+    for (u32 t = t0; t < t0 + per && t < wt; t++) sum += hist[t];
+    u32 incl = sum;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const u32 v = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= (u32)d) incl += v;
+    }
+    if (lane == 31) s_wsum[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        const u32 v = lane < SC_THREADS / 32 ? s_wsum[lane] : 0u;
+        u32 iv = v;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const u32 u = __shfl_up_sync(0xffffffffu, iv, d);
+            if (lane >= (u32)d) iv += u;
+        }
+        if (lane < SC_THREADS / 32) s_wsum[lane] = iv - v;
+    }
+    __syncthreads();
+    // reserve each tile's run in its bucket; hist becomes the placement cursor and gb the
+    // bucket slot of sorted index 0 of that run (mod 2^32)
+    u32 start = s_wsum[warp] + incl - sum;
+    for (u32 t = t0; t < t0 + per && t < wt; t++) {
+        const u32 c = hist[t];
+        if (c) {
+            const u32 g = atomicAdd(a.cnt + t, c);
+            if (g + c > a.cap) atomicOr(a.err, 2u);
+            gb[t] = g - start;
+        }
+        hist[t] = start;
+        start += c;
+    }
+    __syncthreads();
+    for (u32 i = tid; i < n; i += SC_THREADS) {
+        const u32 r = stage[i];
+        sorted[atomicAdd(&hist[r >> SC_OFF_BITS], 1u)] = r;
+    }
+    __syncthreads();
+    // the runs of one tile are consecutive in sorted order and in the bucket
+    for (u32 i = tid; i < n; i += SC_THREADS) {
+        const u32 r = sorted[i], tl = r >> SC_OFF_BITS, slot = gb[tl] + i;
+        if (slot < a.cap) a.rec[(u64)tl * a.cap + slot] = r & ((1u << SC_OFF_BITS) - 1u);
+    }
+    __syncthreads();
+    for (u32 t = tid; t < wt; t += SC_THREADS) hist[t] = 0;
+    if (tid == 0) *s_fill = 0;
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(SC_THREADS, 2) scatter_kernel(ScatterArgs a)
+{
+    extern __shared__ __align__(16) u32 ssm[];
+    u32 *stage = ssm, *sorted = ssm + SC_STAGE, *hist = ssm + 2 * SC_STAGE, *gb = hist + a.wt;
+    __shared__ u32 s_fill;
+    __shared__ u32 s_wsum[SC_THREADS / 32];
+    const u32 tid = threadIdx.x, lane = tid & 31, wt = a.wt, tlog = a.tlog, tmask = (1u << tlog) - 1;
+    for (u32 i = tid; i < wt; i += SC_THREADS) hist[i] = 0;
+    if (tid == 0) s_fill = 0;
+    const u64 wstart = (u64)a.t0 << tlog;
+    u64 wend = (u64)(a.t0 + wt) << tlog;
     if (wend > a.nbx) wend = a.nbx;
     u64 wend_halo = wend + HALO_BITS;
     if (wend_halo > a.nbx) wend_halo = a.nbx;
     const u64 x0 = a.base + 2 * wstart + 1;
-    const u32 k0 = __ldg(a.bounds + blockIdx.x), k1 = __ldg(a.bounds + blockIdx.x + 1);
-    const u32 span = (u32)(wend_halo - wstart);        // < 2^31 (checked by the planner)
     const u32 xm = (u32)(x0 % 30u);
-    for (u32 k = k0 + tid; k < k1; k += nth) scatter_prime<0>(a, k, x0, xm, span, scnt, sbase);
+    const u32 span = (u32)(wend_halo - wstart);          // < 2^31 (checked by the planner)
+    const u32 k1 = __ldg(a.bounds + blockIdx.x + 1);
+    u32 k = __ldg(a.bounds + blockIdx.x) + tid;
+    u32 jj[8], turn = 0;
+    bool have = false;
     __syncthreads();
-    for (u32 i = tid; i < a.wt; i += nth) {
-        const u32 c = scnt[i];
-        sbase[i] = c ? atomicAdd(a.cnt + i, c) : 0;
-        scnt[i] = 0;
+    for (;;) {
+        while (!have && k < k1) {
+            have = scatter_setup(a, k, x0, xm, span, jj, turn);
+            k += SC_THREADS;
+        }
+        if (!__syncthreads_or(have)) break;
+        if (s_fill > SC_STAGE - 8 * SC_THREADS)            // the same value in every thread
+            scatter_flush(a, stage, sorted, hist, gb, &s_fill, s_wsum);
+        // one turn of the wheel: up to 8 records
+        u32 rec[8], nmine = 0;
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            const bool v = have && jj[i] < span;
+            const u32 tl = jj[i] >> tlog, off = jj[i] & tmask;
+            const bool own = v && tl < wt;
+            rec[i] = own ? (tl << SC_OFF_BITS) | off : 0xffffffffu;
+            nmine += own;
+            if (v && off < HALO_BITS && tl >= 1 && tl - 1 < wt) {     // halo copy for tile tl - 1
+                const u32 slot = atomicAdd(a.cnt + tl - 1, 1u);
+                if (slot < a.cap) a.rec[(u64)(tl - 1) * a.cap + slot] = off + (1u << tlog);
+                else atomicOr(a.err, 2u);
+            }
+            jj[i] = v ? jj[i] + turn : span;
+        }
+        have = have && jj[0] < span;
+        // warp-aggregated append to the stage
+        u32 incl = nmine;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const u32 u = __shfl_up_sync(0xffffffffu, incl, d);
+            if (lane >= (u32)d) incl += u;
+        }
+        u32 base = 0;
+        if (lane == 31) base = atomicAdd(&s_fill, incl);
+        base = __shfl_sync(0xffffffffu, base, 31);
+        u32 pos = base + incl - nmine;
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            if (rec[i] != 0xffffffffu) {
+                stage[pos++] = rec[i];
+                atomicAdd(&hist[rec[i] >> SC_OFF_BITS], 1u);
+            }
+        }
     }
-    __syncthreads();
-    for (u32 k = k0 + tid; k < k1; k += nth) scatter_prime<1>(a, k, x0, xm, span, scnt, sbase);
+    scatter_flush(a, stage, sorted, hist, gb, &s_fill, s_wsum);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -1075,6 +1150,7 @@ static int plan_sieve(mp_handle *h, const PrimeTable &tb, u64 lo, u64 hi, u32 tl
         if (wt > wmem) wt = wmem;
         if (wt < 1) wt = 1;
         if (wt > P.g.ntiles) wt = P.g.ntiles;
+        if (wt > 2048) wt = 2048;                  // the scatter's staged records keep 11 bits of tile
         while (wt > 1 && (wt << tlog) + HALO_BITS >= (1ull << 31)) wt /= 2;   // 32-bit wave positions
         P.wt = (u32)wt;
         P.nwaves = (P.g.ntiles + P.wt - 1) / P.wt;
@@ -1094,50 +1170,51 @@ static void fill_tile_args(mp_handle *h, const PrimeTable &tb, const SievePlan &
     for (int p = 0; p < MP_NPAT; p++) { a.pat[p] = h->pat.d_words[p]; a.period[p] = h->pat.period[p]; }
 }
 
-// CTA boundaries for the scatter kernel: contiguous runs of the large primes [i0, i1) with
-// equal shares of the sum of 1/q (the expected hits per wave), so that the CTAs of the small
-// large primes, which hit far more often, get proportionally fewer primes.  Built on the host
-// from the table's prefix sums and uploaded once per prime range (never inside a capture).
+static cudaError_t launch_scatter(const ScatterArgs &s, u32 nblk, cudaStream_t st)
+{
+    const size_t smem = ((size_t)2 * SC_STAGE + 2 * s.wt) * 4;
+    static bool attr_set[16] = {false};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 16) return cudaErrorInvalidDevice;
+    if (!attr_set[dev]) {
+        // the largest wave (2048 tiles)
+        cudaError_t e = cudaFuncSetAttribute(scatter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)(((size_t)2 * SC_STAGE + 2 * 2048) * 4));
+        if (e != cudaSuccess) return e;
+        attr_set[dev] = true;
+    }
+    scatter_kernel<<<nblk, SC_THREADS, smem, st>>>(s);
+    return cudaGetLastError();
+}
+
+// CTA boundaries for the scatter kernel: contiguous runs of the large primes [i0, i1) of equal
+// work, where a prime's work is its expected hits in a wave (proportional to 1/q) plus its
+// set-up, worth about 8 hits in a wave of 2^30 bits.  Two persistent CTAs per SM.  Built on
+// the host from the table's prefix sums of 1/q and uploaded once per prime range (never
+// inside a capture).
 static int scatter_bounds(mp_handle *h, const PrimeTable &tb, u32 i0, u32 i1, cudaStream_t st)
 {
-    const u32 want = (u32)std::max<u64>(1, std::min<u64>((u64)h->sm_count * 16, i1 - i0));
+    const u32 want = (u32)std::max<u64>(1, std::min<u64>((u64)h->sm_count * 2, i1 - i0));
     if (h->scat_key[0] == i0 && h->scat_key[1] == i1 && h->scat_key[2] == want && h->scat_nblk) return MP_OK;
+    if (tb.inv_prefix.size() < (size_t)i1 + 1) return mp_set_error(h, MP_EINVAL, "prime table has no prefix sums");
+    const double c = 8.0 / ((double)(1u << 30) * 8.0 / 15.0);      // set-up, in units of 1/q
+    auto W = [&](u32 i) { return tb.inv_prefix[i] + c * i; };
     std::vector<u32> &b = h->scat_host;
     b.clear();
     b.push_back(i0);
-    if (!tb.work_bounds.empty()) {
-        // the table's equal-work cut points inside (i0, i1), then halve the widest runs until
-        // there are enough CTAs
-        auto a = std::upper_bound(tb.work_bounds.begin(), tb.work_bounds.end(), i0);
-        auto z = std::lower_bound(tb.work_bounds.begin(), tb.work_bounds.end(), i1);
-        for (auto it = a; it != z; ++it) b.push_back(*it);
-        b.push_back(i1);
-        while (b.size() - 1 < want) {
-            std::vector<u32> c;
-            c.push_back(b[0]);
-            bool grew = false;
-            for (size_t k = 1; k < b.size(); k++) {
-                if (b[k] - b[k - 1] >= 2 && c.size() + (b.size() - k) < (size_t)want + 1) {
-                    c.push_back(b[k - 1] + (b[k] - b[k - 1]) / 2);
-                    grew = true;
-                }
-                c.push_back(b[k]);
-            }
-            b.swap(c);
-            if (!grew) break;
+    const double w0 = W(i0), w1 = W(i1);
+    for (u32 n = 1; n < want; n++) {
+        const double target = w0 + (w1 - w0) * n / want;
+        u32 lo = b.back() + 1, hi = i1;                               // first i with W(i) >= target
+        while (lo < hi) {
+            const u32 mid = lo + (hi - lo) / 2;
+            if (W(mid) < target) lo = mid + 1; else hi = mid;
         }
-    } else {
-        const double p0 = tb.inv_prefix[i0], p1 = tb.inv_prefix[i1];
-        for (u32 c = 1; c < want; c++) {
-            const double target = p0 + (p1 - p0) * c / want;
-            u32 k = (u32)(std::lower_bound(tb.inv_prefix.begin() + i0, tb.inv_prefix.begin() + i1, target) -
-                          tb.inv_prefix.begin());
-            if (k <= b.back()) k = b.back() + 1;
-            if (k >= i1) break;
-            b.push_back(k);
-        }
-        b.push_back(i1);
+        if (lo >= i1) break;
+        b.push_back(lo);
     }
+    b.push_back(i1);
     MP_CUDA(h, h->scat_bounds.ensure(b.size() * 4));
     MP_CUDA(h, cudaMemcpyAsync(h->scat_bounds.p, b.data(), b.size() * 4, cudaMemcpyHostToDevice, st));
     MP_CUDA(h, cudaStreamSynchronize(st));
@@ -1178,9 +1255,8 @@ static int run_tiles(mp_handle *h, const PrimeTable &tb, const SievePlan &P, Til
             const u32 nblk = h->scat_nblk;
             {
                 ProfScope ps(h, PROF_SCATTER, st);
-                scatter_kernel<<<nblk, 512, (size_t)nt * 8, st>>>(s);
+                MP_CUDA(h, launch_scatter(s, nblk, st));
             }
-            MP_CUDA(h, cudaGetLastError());
             a.rec = s.rec; a.reccnt = s.cnt; a.reccap = P.cap;
         }
         a.t0 = t0; a.nt = nt;
@@ -1269,19 +1345,6 @@ int mp_tables_ensure(mp_handle *h, u64 limit)
     h->table.inv_prefix.resize(total + 1);
     h->table.inv_prefix[0] = 0.0;
     for (u64 i = 0; i < total; i++) h->table.inv_prefix[i + 1] = h->table.inv_prefix[i] + 1.0 / h->table.host[i];
-    {
-        // 32768 runs of equal sum 1/q over the whole table (the scatter CTAs of any prime range
-        // are cut from these)
-        const int NB = 32768;
-        h->table.work_bounds.clear();
-        const double P = h->table.inv_prefix[total];
-        for (int c = 1; c < NB; c++) {
-            const u64 k = (u64)(std::lower_bound(h->table.inv_prefix.begin(), h->table.inv_prefix.end(), P * c / NB) -
-                                h->table.inv_prefix.begin());
-            if (k < total && (h->table.work_bounds.empty() || k > h->table.work_bounds.back()))
-                h->table.work_bounds.push_back((u32)k);
-        }
-    }
     h->scat_key[0] = ~0ull;
     MP_TRY(check_errflag(h, st));
     h->table.n = total;
