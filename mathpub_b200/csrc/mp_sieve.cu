@@ -312,7 +312,9 @@ __global__ void __launch_bounds__(1024) tile_kernel(TileArgs a)
                     atomicOr(&sm[j >> 5], 1u << (j & 31));
             }
         }
-        // 4. large primes: bucket records of this tile
+        // 4. large primes: bucket records of this tile.  Records and bitmap words are read or
+        //    written once, with streaming cache hints, so that the prime table and the carried
+        //    state of the sparse primes stay in L2.
         if (a.rec) {
             u32 n = __ldg(a.reccnt + rel);
             if (n > a.reccap) n = a.reccap;
@@ -321,22 +323,22 @@ __global__ void __launch_bounds__(1024) tile_kernel(TileArgs a)
             const u32 n4 = n >> 2;
             u32 i = tid;
             for (; i + 3 * nth < n4; i += 4 * nth) {             // 16 records in flight per thread
-                const uint4 r0 = __ldg(R4 + i), r1 = __ldg(R4 + i + nth);
-                const uint4 r2 = __ldg(R4 + i + 2 * nth), r3 = __ldg(R4 + i + 3 * nth);
+                const uint4 r0 = __ldcs(R4 + i), r1 = __ldcs(R4 + i + nth);
+                const uint4 r2 = __ldcs(R4 + i + 2 * nth), r3 = __ldcs(R4 + i + 3 * nth);
                 const u32 js[16] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w,
                                     r2.x, r2.y, r2.z, r2.w, r3.x, r3.y, r3.z, r3.w};
 #pragma unroll
                 for (int k = 0; k < 16; k++) atomicOr(&sm[js[k] >> 5], 1u << (js[k] & 31));
             }
             for (; i < n4; i += nth) {
-                const uint4 r0 = __ldg(R4 + i);
+                const uint4 r0 = __ldcs(R4 + i);
                 atomicOr(&sm[r0.x >> 5], 1u << (r0.x & 31));
                 atomicOr(&sm[r0.y >> 5], 1u << (r0.y & 31));
                 atomicOr(&sm[r0.z >> 5], 1u << (r0.z & 31));
                 atomicOr(&sm[r0.w >> 5], 1u << (r0.w & 31));
             }
             for (u32 k = (n4 << 2) + tid; k < n; k += nth) {
-                const u32 j = __ldg(R + k);
+                const u32 j = __ldcs(R + k);
                 atomicOr(&sm[j >> 5], 1u << (j & 31));
             }
         }
@@ -495,7 +497,7 @@ __global__ void __launch_bounds__(1024) tile_kernel(TileArgs a)
                 for (u32 w = tid; w < TW; w += nth) {
                     const u64 bit0 = G + 32ull * w;
                     if (bit0 >= lim64) break;
-                    a.bitmap32[(G >> 5) + w] = ~sm[w] & bits_mask(bit0, limit);
+                    __stcs(a.bitmap32 + (G >> 5) + w, ~sm[w] & bits_mask(bit0, limit));
                 }
             }
         } else {
@@ -570,10 +572,18 @@ struct ScatterArgs {
 // warp.  When the stage is nearly full the CTA sorts it by tile (counting sort), reserves one
 // run per tile in the bucket with one global atomic, and writes the runs out, so that the
 // record stores of a warp are coalesced.  Halo copies (one hit in 1024) go to the bucket
-// directly.
+// directly.  Measured on B200 at 1e15 (2^34 integers): stage 8192 with three CTAs per SM
+// 4.36 ms, 12288 with two 4.58 ms, 24576 with one 6.4 ms (5.0 ms with 1024 threads).
 
+#ifndef SC_THREADS
 #define SC_THREADS 512
-#define SC_STAGE 12288                    // staged records per CTA; two CTAs per SM
+#endif
+#ifndef SC_STAGE
+#define SC_STAGE 8192                     // staged records per CTA (two buffers of them)
+#endif
+#ifndef SC_CTAS_PER_SM
+#define SC_CTAS_PER_SM 3                  // 48 warps per SM: the walk is latency-bound
+#endif
 #define SC_OFF_BITS 21                    // staged record: tile << 21 | offset (offset < 2^21)
 
 // set up prime k: the 8 progression starts (ascending, below j + 15 q) relative to the wave;
@@ -654,7 +664,7 @@ __device__ __forceinline__ void scatter_flush(const ScatterArgs &a, u32 *stage, 
     // the runs of one tile are consecutive in sorted order and in the bucket
     for (u32 i = tid; i < n; i += SC_THREADS) {
         const u32 r = sorted[i], tl = r >> SC_OFF_BITS, slot = gb[tl] + i;
-        if (slot < a.cap) a.rec[(u64)tl * a.cap + slot] = r & ((1u << SC_OFF_BITS) - 1u);
+        if (slot < a.cap) __stcs(a.rec + (u64)tl * a.cap + slot, r & ((1u << SC_OFF_BITS) - 1u));
     }
     __syncthreads();
     for (u32 t = tid; t < wt; t += SC_THREADS) hist[t] = 0;
@@ -662,7 +672,7 @@ __device__ __forceinline__ void scatter_flush(const ScatterArgs &a, u32 *stage, 
     __syncthreads();
 }
 
-__global__ void __launch_bounds__(SC_THREADS, 2) scatter_kernel(ScatterArgs a)
+__global__ void __launch_bounds__(SC_THREADS, SC_CTAS_PER_SM) scatter_kernel(ScatterArgs a)
 {
     extern __shared__ __align__(16) u32 ssm[];
     u32 *stage = ssm, *sorted = ssm + SC_STAGE, *hist = ssm + 2 * SC_STAGE, *gb = hist + a.wt;
@@ -689,8 +699,12 @@ __global__ void __launch_bounds__(SC_THREADS, 2) scatter_kernel(ScatterArgs a)
             have = scatter_setup(a, k, x0, xm, span, jj, turn);
             k += SC_THREADS;
         }
-        if (!__syncthreads_or(have)) break;
-        if (s_fill > SC_STAGE - 8 * SC_THREADS)            // the same value in every thread
+        if (!__syncthreads_or(have)) break;                // the last round's appends are done
+        // every thread takes the fill before any thread appends again, so the flush decision
+        // (and the barriers inside the flush) is the same in every thread
+        const u32 fill = s_fill;
+        __syncthreads();
+        if (fill > SC_STAGE - 8 * SC_THREADS)
             scatter_flush(a, stage, sorted, hist, gb, &s_fill, s_wsum);
         // one turn of the wheel: up to 8 records
         u32 rec[8], nmine = 0;
@@ -703,7 +717,7 @@ __global__ void __launch_bounds__(SC_THREADS, 2) scatter_kernel(ScatterArgs a)
             nmine += own;
             if (v && off < HALO_BITS && tl >= 1 && tl - 1 < wt) {     // halo copy for tile tl - 1
                 const u32 slot = atomicAdd(a.cnt + tl - 1, 1u);
-                if (slot < a.cap) a.rec[(u64)(tl - 1) * a.cap + slot] = off + (1u << tlog);
+                if (slot < a.cap) __stcs(a.rec + (u64)(tl - 1) * a.cap + slot, off + (1u << tlog));
                 else atomicOr(a.err, 2u);
             }
             jj[i] = v ? jj[i] + turn : span;
@@ -919,14 +933,14 @@ __global__ void __launch_bounds__(32) hash_kernel(const u32 *__restrict__ bm, u6
         const uint4 *v = (const uint4 *)(p + k);
         uint4 buf[HASH_AHEAD];
 #pragma unroll
-        for (int i = 0; i < HASH_AHEAD; i++) buf[i] = __ldg(v + i);
+        for (int i = 0; i < HASH_AHEAD; i++) buf[i] = __ldcs(v + i);
         for (u64 b = 0; b < nblk; b++) {
             const uint4 *nx = v + (b + 1) * HASH_AHEAD;
             const bool more = b + 1 < nblk;
 #pragma unroll
             for (int i = 0; i < HASH_AHEAD; i++) {
                 const uint4 x = buf[i];
-                if (more) buf[i] = __ldg(nx + i);
+                if (more) buf[i] = __ldcs(nx + i);
                 fnv_16(h, x);
             }
         }
@@ -934,7 +948,7 @@ __global__ void __launch_bounds__(32) hash_kernel(const u32 *__restrict__ bm, u6
     }
     // the rest in 16-byte words while one byte more remains, then bytes; the last byte keeps
     // only the bits of the segment
-    for (; k + 16 < nbytes; k += 16) fnv_16(h, __ldg((const uint4 *)(p + k)));
+    for (; k + 16 < nbytes; k += 16) fnv_16(h, __ldcs((const uint4 *)(p + k)));
     for (; k < nbytes; k++) {
         u8 c = p[k];
         const u64 rem = len - 8 * k;
@@ -1190,12 +1204,12 @@ static cudaError_t launch_scatter(const ScatterArgs &s, u32 nblk, cudaStream_t s
 
 // CTA boundaries for the scatter kernel: contiguous runs of the large primes [i0, i1) of equal
 // work, where a prime's work is its expected hits in a wave (proportional to 1/q) plus its
-// set-up, worth about 8 hits in a wave of 2^30 bits.  Two persistent CTAs per SM.  Built on
+// set-up, worth about 8 hits in a wave of 2^30 bits.  SC_CTAS_PER_SM persistent CTAs per SM.  Built on
 // the host from the table's prefix sums of 1/q and uploaded once per prime range (never
 // inside a capture).
 static int scatter_bounds(mp_handle *h, const PrimeTable &tb, u32 i0, u32 i1, cudaStream_t st)
 {
-    const u32 want = (u32)std::max<u64>(1, std::min<u64>((u64)h->sm_count * 2, i1 - i0));
+    const u32 want = (u32)std::max<u64>(1, std::min<u64>((u64)h->sm_count * SC_CTAS_PER_SM, i1 - i0));
     if (h->scat_key[0] == i0 && h->scat_key[1] == i1 && h->scat_key[2] == want && h->scat_nblk) return MP_OK;
     if (tb.inv_prefix.size() < (size_t)i1 + 1) return mp_set_error(h, MP_EINVAL, "prime table has no prefix sums");
     const double c = 8.0 / ((double)(1u << 30) * 8.0 / 15.0);      // set-up, in units of 1/q
