@@ -243,17 +243,28 @@ __global__ void __launch_bounds__(1024) tile_kernel(TileArgs a)
 
         // multiples q k with k coprime to 30 only (wheel of 30; the patterns hold 3 and 5)
         const u32 xm = (u32)(x0 % 30u);
-        // 2. warp tier: one warp per prime; lane l walks residue (l & 7) of the wheel in turn
-        //    (l >> 3), four turns (60 q bits) per step
-        for (u32 k = a.iw0 + warp; k < a.iw1; k += nwarps) {
-            const u32 q = __ldg(a.q + k);
-            const u32 r = mp_mod_barrett(x0, q, __ldg(a.magic + k));
-            const u64 j64 = mp_first_odd_multiple(x0, q, r, NB);
-            if (j64 >= NB) continue;
-            u32 w;
-            const u32 jw = (u32)mp_w30_first((u32)j64, xm, q, &w);
-            const u32 j0 = jw + q * (mp_w30_span(mp_w30_steps(w), lane & 7) + 15u * (lane >> 3));
-            for (u32 j = j0; j < NB; j += 60u * q) atomicOr(&sm[j >> 5], 1u << (j & 31));
+        // 2. warp tier.  Warp w takes the primes w, w + nwarps, w + 2 nwarps, ... of the tier
+        //    (equal shares of the marks), 32 at a time: lane i sets up prime i of the batch
+        //    (first multiple and wheel index), then the warp marks the batch one prime after the
+        //    other, lane l walking residue (l & 7) of the wheel in turn (l >> 3), four turns
+        //    (60 q bits) per step.
+        for (u32 kb = a.iw0 + warp; kb < a.iw1; kb += 32 * nwarps) {
+            const u32 k = kb + nwarps * lane;
+            u32 q = 0, jw = NB, w = 0;                         // jw >= NB: nothing to mark
+            if (k < a.iw1) {
+                q = __ldg(a.q + k);
+                const u32 r = mp_mod_barrett(x0, q, __ldg(a.magic + k));
+                const u64 j64 = mp_first_odd_multiple(x0, q, r, NB);
+                if (j64 < NB) jw = (u32)mp_w30_first((u32)j64, xm, q, &w);
+            }
+            const u32 n = min(32u, (a.iw1 - kb + nwarps - 1) / nwarps);
+            for (u32 i = 0; i < n; i++) {
+                const u32 qi = __shfl_sync(0xffffffffu, q, i), ji = __shfl_sync(0xffffffffu, jw, i);
+                const u32 wi = __shfl_sync(0xffffffffu, w, i);
+                if (ji >= NB) continue;
+                const u32 j0 = ji + qi * (mp_w30_span(mp_w30_steps(wi), lane & 7) + 15u * (lane >> 3));
+                for (u32 j = j0; j < NB; j += 60u * qi) atomicOr(&sm[j >> 5], 1u << (j & 31));
+            }
         }
         // 3. thread tier, one thread per prime.  Dense primes (q < T / 32) have several
         //    multiples per residue of the wheel in a tile: set up from x0 in every tile and
