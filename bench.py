@@ -42,6 +42,9 @@ BLOCK_LOG2 = 24
 HASH_LOG2 = 20
 BPSW_SEED, BPSW_COUNT, BPSW_LISTS = 0x3C0FFEE, 1 << 26, 4096
 HBM_FALLBACK_GBS = 6650.0
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one tile-kernel launch (a wave
+# of 1184 tiles at 1e15), from an ncu capture of that launch
+TILE_TRAFFIC_BYTES = 597.8e6 + 293.2e6
 WORKLOAD = ("large-offset sieve [1e15, 1e15+2^34) per GPU, odd-only bitmap, sieving primes up to 31623048, "
             "wheel/pattern presieve 3..89, bucket sieve above the tile; outputs per-2^24-block pi, twins, "
             "6-tuples {0,4,6,10,12,16} with checksum, max gap + start, per-2^20 FNV-1a bitmap hashes")
@@ -71,7 +74,7 @@ class ClockSampler:
     def start(self):
         try:
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
-                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                       "--format=csv,noheader,nounits", "-lms", "50"],
                                       stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.p = None
@@ -321,11 +324,13 @@ def run_ours(args):
                     "api": "mp_sieve_range (host buffers)"},
             "gpu_launches": launches_per_step * args.steps,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                         "frac": achieved / hbm, "traffic": None, "kernel": f"tile_kernel<{tile_bits.bit_length() - 1},0>",
+                         "frac": achieved / hbm, "traffic": TILE_TRAFFIC_BYTES,
+                         "kernel": f"tile_kernel<{tile_bits.bit_length() - 1},0>",
                          "peak_source": f"{hbm_src} (MEASURED_PEAKS.json hbm_gbs)" if hbm_src == "measured" else "fallback",
                          "algorithmic_bytes_per_launch": tile_bytes, "avg_launch_ms": tile_avg_s * 1e3,
-                         "note": "bytes = bucket records read (4 B per large-prime hit) + bitmap written; "
-                                 "the binding resource is shared-memory atomics, see roofline_smem"},
+                         "note": "bytes = bucket records read (4 B per large-prime hit) + bitmap written; traffic = "
+                                 "DRAM bytes of one launch from an ncu capture; the kernel is bound by instruction "
+                                 "issue and shared-memory atomics, see roofline_smem"},
             "roofline_smem": {"bound": "smem_atomics", "achieved": smem_marks_rate,
                               "peak": peaks["smem_atomic_conflict_free"], "unit": "atomic ops/s",
                               "frac": smem_marks_rate / peaks["smem_atomic_conflict_free"],
