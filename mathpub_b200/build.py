@@ -14,7 +14,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmathpub.so")
 WORK = os.path.join(HERE, "libmpwork.so")
-SOURCES = ["mp_api.cu", "mp_sieve.cu", "mp_bpsw.cu", "mp_fermat.cu", "mp_tune.cu", "mp_serve.cu", "mp_probe.cu"]
+SOURCES = ["mp_api.cu", "mp_sieve.cu", "mp_bpsw.cu", "mp_fermat.cu", "mp_tune.cu", "mp_serve.cu", "mp_probe.cu",
+           "mp_primesieve.cu"]
 HEADERS = ["mp_common.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = [
@@ -29,7 +30,8 @@ def _stale():
     if not os.path.exists(LIB):
         return True
     t = os.path.getmtime(LIB)
-    deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS] + [os.path.join(ROOT, "include", "mathpub_gpu.h")]
+    deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS] + [os.path.join(ROOT, "include", h)
+                                                                  for h in ("mathpub_gpu.h", "primesieve.h")]
     return any(os.path.getmtime(d) > t for d in deps)
 
 
