@@ -120,6 +120,30 @@ int mp_sieve_range_dev(mp_handle *h, uint64_t lo, uint64_t hi, const mp_sieve_op
 int mp_primes_range(mp_handle *h, uint64_t lo, uint64_t hi, uint64_t *primes, size_t cap,
                     size_t *count);
 
+/* ---- gap statistics: consumers of the per-prime gap stream ----
+ * For the primes p in [lo, hi), with the primes after p = q_1 < q_2 < ... and gaps
+ * g_1 = q_1 - p, g_i = q_i - q_(i-1):
+ *   gap_hist[g / 2]   primes whose gap g_1 is the even g (gap_hist[0] holds the gap 1 of
+ *                     p = 2); the power sums T_k = sum of count(g) g^k of A252768 come from it
+ *                     (A252768/README.md:386-425: the chunk totals of its ordered hand-off)
+ *   run_hist[L]       primes with L(p) = L, L(p) = the largest n with g_1 < g_2 < ... < g_n
+ *                     (A158939/a158939.c:17-30; L >= 1; run_hist[0] stays 0)
+ *   run_first[L]      the smallest such prime, 0 if none (A158939's a(L))
+ *   unsettled         primes whose run goes on past the look-ahead of 2^16 integers after hi
+ *                     (not counted in run_hist; none below 2^64 is known)
+ * Replaces the per-prime walks of A158939/a158939.c:720-770 (its chunk scan) and the gap
+ * histogram of A252768/a252768.c (its chunk totals).  hi <= 2^64 - 2^18 - 2^17. */
+#define MP_GAP_BINS 1024
+#define MP_RUN_MAX 64
+typedef struct {
+    uint64_t gap_hist[MP_GAP_BINS];
+    uint64_t run_hist[MP_RUN_MAX];
+    uint64_t run_first[MP_RUN_MAX];
+    uint64_t unsettled;
+} mp_gap_stats;
+
+int mp_gap_stats_range(mp_handle *h, uint64_t lo, uint64_t hi, mp_gap_stats *out);
+
 /* ---- BPSW ----
  * verdict bit i (bit i & 7 of byte i >> 3) = 1 iff n[i] is prime.  For n < 2^64 this is
  * BPSW (base-2 strong test + strong Lucas test with Selfridge's parameters) after trial

@@ -64,6 +64,19 @@ class ServeResult(C.Structure):
                 ("submit_s", C.c_double), ("done_s", C.c_double)]
 
 
+GAP_BINS, RUN_MAX = 1024, 64
+
+
+class GapStats(C.Structure):
+    _fields_ = [("gap_hist", C.c_uint64 * GAP_BINS), ("run_hist", C.c_uint64 * RUN_MAX),
+                ("run_first", C.c_uint64 * RUN_MAX), ("unsettled", C.c_uint64)]
+
+    def as_dict(self):
+        return {"gap_hist": np.ctypeslib.as_array(self.gap_hist).copy(),
+                "run_hist": np.ctypeslib.as_array(self.run_hist).copy(),
+                "run_first": np.ctypeslib.as_array(self.run_first).copy(), "unsettled": int(self.unsettled)}
+
+
 class MathpubError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"{_ERRNAMES.get(code, code)}: {msg}")
@@ -101,6 +114,7 @@ def lib():
             "mp_fermat_q_base2_dev": ([vp, vp, C.c_size_t, vp, vp], C.c_int),
             "mp_wieferich_range": ([vp, u64, u64, vp], C.c_int),
             "mp_wieferich_stats_noalloc": ([vp, vp, u64, vp, vp], C.c_int),
+            "mp_gap_stats_range": ([vp, u64, u64, vp], C.c_int),
             "mp_autotune": ([vp, u64, C.c_char_p, C.c_size_t], C.c_int),
             "mp_profile_enable": ([vp, C.c_int], C.c_int),
             "mp_profile_read": ([vp, vp, vp, C.c_int], C.c_int),
@@ -239,6 +253,13 @@ class Engine:
         q = np.zeros(len(p), dtype=np.uint64)
         self._check(lib().mp_fermat_q_base2(self._h, _p(p), len(p), _p(q)))
         return q
+
+    def gap_stats(self, lo, hi):
+        """Gap histogram and A158939 run statistics of the primes in [lo, hi)
+        (mp_gap_stats_range)."""
+        g = GapStats()
+        self._check(lib().mp_gap_stats_range(self._h, lo, hi, C.byref(g)))
+        return g.as_dict()
 
     def wieferich_range(self, lo, hi):
         out = WiefStats()

@@ -54,7 +54,6 @@ void mp_graphs_free(mp_handle *h)
     h->graphs = nullptr;
 }
 
-int mp_sieve_errors(mp_handle *h, cudaStream_t st);   // mp_sieve.cu
 
 extern "C" {
 
@@ -85,7 +84,7 @@ int mp_init(int device, mp_handle **out)
     h->graphs = new GraphCache();
     DevBuf *bufs[] = {&h->tilesum, &h->blockacc, &h->rec, &h->reccnt, &h->queue, &h->errflag, &h->scratch_bitmap,
                       &h->bpsw_n, &h->bpsw_bits, &h->ferm_p, &h->ferm_q, &h->ferm_part, &h->stats_out, &h->small_out,
-                      &h->boot.q, &h->boot.magic, &h->table.q, &h->table.magic, &h->scat_bounds, &h->tstate};
+                      &h->boot.q, &h->boot.magic, &h->table.q, &h->table.magic, &h->scat_bounds, &h->tstate, &h->gap_acc};
     for (DevBuf *b : bufs) b->gen = &h->buf_gen;
     *out = h;
     return MP_OK;
@@ -99,7 +98,7 @@ int mp_free(mp_handle *h)
     mp_graphs_free(h);
     DevBuf *bufs[] = {&h->tilesum, &h->blockacc, &h->rec, &h->reccnt, &h->queue, &h->errflag, &h->scratch_bitmap,
                       &h->bpsw_n, &h->bpsw_bits, &h->ferm_p, &h->ferm_q, &h->ferm_part, &h->stats_out, &h->small_out,
-                      &h->boot.q, &h->boot.magic, &h->table.q, &h->table.magic, &h->scat_bounds, &h->tstate};
+                      &h->boot.q, &h->boot.magic, &h->table.q, &h->table.magic, &h->scat_bounds, &h->tstate, &h->gap_acc};
     for (DevBuf *b : bufs) b->release();
     for (int p = 0; p < MP_NPAT; p++)
         if (!h->shared_tables && h->pat_ready && h->pat.d_words[p]) cudaFree(h->pat.d_words[p]);

@@ -202,7 +202,7 @@ struct mp_handle {
 
     // scratch
     DevBuf tilesum, blockacc, rec, reccnt, queue, errflag, scratch_bitmap, bpsw_n, bpsw_bits,
-        ferm_p, ferm_q, ferm_part, stats_out, small_out, scat_bounds, tstate;
+        ferm_p, ferm_q, ferm_part, stats_out, small_out, scat_bounds, tstate, gap_acc;
     u64 scat_key[3] = {~0ull, ~0ull, ~0ull};   // (first, end, blocks) the bounds were built for
     std::vector<u32> scat_host;
     u32 scat_nblk = 0;
@@ -287,6 +287,7 @@ int mp_sieve_run(mp_handle *h, u64 lo, u64 hi, const mp_sieve_opts *o, mp_range_
                  mp_block_stats *d_blocks, u64 *d_hash, u64 *d_bitmap, cudaStream_t st);
 int mp_sieve_emit_primes(mp_handle *h, u64 lo, u64 hi, u64 *d_primes, u64 cap, u64 *count,
                          cudaStream_t st);                           // synchronises
+int mp_sieve_errors(mp_handle *h, cudaStream_t st);                  // synchronises; reads the error flag
 int mp_bpsw_run(mp_handle *h, const u64 *d_n, const u64 *offs, const u32 *lens, u32 nlists,
                 u32 *d_bits, u32 mode, cudaStream_t st);             // mp_bpsw.cu
 int mp_fermat_run(mp_handle *h, const u64 *d_p, u64 count, u64 *d_q, cudaStream_t st,

@@ -201,3 +201,43 @@ def ref_wieferich_scan(lo, hi, nthreads=None):
 
 def mix64(z):
     return int(o().or_mix64(z))
+
+
+GAP_BINS, RUN_MAX, GAP_LOOK = 1024, 64, 1 << 16
+
+
+def gap_stats(lo, hi, nthreads=None):
+    """Statistics of the gaps that follow the primes p in [lo, hi) (the primes after hi come
+    from a look-ahead of 2^16 integers):
+      gap_hist[g // 2]  primes whose next gap is g (the gap 1 of p = 2 in bin 0);
+      run_hist[L]       primes with L(p) = L, the number of strictly increasing gaps that
+                        follow p (A158939/a158939.c:17-30: L(p) = largest n with
+                        g_1 < g_2 < ... < g_n);
+      run_first[L]      the smallest such p (0 if none): A158939's a(L) on [lo, hi);
+      unsettled         primes whose run is still increasing at the end of the look-ahead.
+    Computed from the oracle's prime list."""
+    p = primes_range(lo, hi + GAP_LOOK, nthreads).astype(np.int64)
+    n_in = int(np.searchsorted(p, hi))
+    g = np.diff(p)                                    # g[i] = gap after p[i]
+    hist = np.zeros(GAP_BINS, dtype=np.uint64)
+    gi = g[:n_in] // 2
+    hist += np.bincount(np.minimum(gi, GAP_BINS - 1), minlength=GAP_BINS).astype(np.uint64)
+    unsettled = n_in - min(n_in, len(g))              # an in-range prime with no next prime
+    # run of p[i]: L = 1 + number of consecutive increases g[i] < g[i+1] < ... ; the run of
+    # p[i] ends at the first j >= i with g[j + 1] <= g[j]
+    stop = np.flatnonzero(g[1:] <= g[:-1])            # j with g[j + 1] <= g[j]
+    idx = np.arange(min(n_in, len(g)))
+    k = np.searchsorted(stop, idx)                    # first stop >= i
+    ended = k < len(stop)
+    L = np.where(ended, stop[np.minimum(k, len(stop) - 1)] - idx + 1 if len(stop) else 0, 0)
+    unsettled += int((~ended).sum())
+    L = L[ended]
+    P = p[:len(idx)][ended]
+    run_hist = np.zeros(RUN_MAX, dtype=np.uint64)
+    run_first = np.zeros(RUN_MAX, dtype=np.uint64)
+    Lc = np.minimum(L, RUN_MAX - 1)
+    run_hist += np.bincount(Lc, minlength=RUN_MAX).astype(np.uint64)
+    for l in range(1, RUN_MAX):                       # P is increasing: the first index is the smallest p
+        if run_hist[l]:
+            run_first[l] = P[int(np.argmax(Lc == l))]
+    return {"gap_hist": hist, "run_hist": run_hist, "run_first": run_first, "unsettled": int(unsettled)}

@@ -36,6 +36,12 @@ static void refill(primesieve_iterator *it)
     }
 }
 
+void primesieve_generate_next_primes(primesieve_iterator *it)
+{
+    refill(it);
+    it->is_error = it->size == 1 && it->primes[0] == PRIMESIEVE_ERROR;
+}
+
 uint64_t primesieve_next_prime(primesieve_iterator *it)
 {
     if (it->i >= it->size) refill(it);

@@ -6,7 +6,8 @@ ref_vectors.json   known answers held by the reference's own sources, extracted 
                    pattern from the files (pseudoprime lists and sextuplet windows of
                    A350826/a350826.c, pi tables and windows of A158939/cuda/a158939_cuda.cu,
                    pi(1e9) of A001220/wieferich.c, twin counts of A007508/README.md, the
-                   base-2 Wieferich primes of A001220/wieferich.c)
+                   base-2 Wieferich primes of A001220/wieferich.c, the known terms of
+                   A158939 (A158939/a158939.c:7-10) and A252768 (A252768/a252768.c:8-9))
 verify_py.json     windows computed by the reference's independent Python verifiers
                    (A001220/verify_wieferich.py, A350826/verify_a350826.py) run here
 configs.json       the full-size workloads computed by the oracle (tests/ checks the oracle
@@ -84,6 +85,12 @@ def ref_vectors():
     r = src("A007508/README.md")
     m = re.search(r"a\(n\) = #.*?\n\n(.*?)\n\n", r, re.S)
     out["twins_below_10n"] = [int(x) for x in re.findall(r"\d+", m.group(1))]
+    g = src("A158939/a158939.c")
+    m = re.search(r"Known terms \(offset 1, n = 1\.\.17\):\n(.*?)\n \* a\(16\)", g, re.S)
+    out["A158939"] = [int(x) for x in re.findall(r"\d+", m.group(1))]
+    g = src("A252768/a252768.c")
+    m = re.search(r"Terms: a\(1\.\.7\) = ([\d, ]+) \(OEIS, 2014\);\n \*\s+a\(8\) = (\d+) and a\(9\) = (\d+)", g)
+    out["A252768"] = [int(x) for x in m.group(1).split(",")] + [int(m.group(2)), int(m.group(3))]
     return out
 
 
