@@ -195,7 +195,7 @@ int mp_wieferich_range(mp_handle *h, uint64_t lo, uint64_t hi, mp_wief_stats *ou
  * memory (`primes` there = count), queued on `stream` (NULL = the legacy default stream).
  * For callers that cannot allocate device memory -- a framework whose allocator owns the
  * whole device, or a loop where a cudaMalloc, which may synchronise, is not allowed -- it
- * allocates nothing and takes no handle.  Its scratch is a fixed array of about 3 MB inside
+ * allocates nothing and takes no handle.  Its scratch is a fixed array of about 400 KB inside
  * the library that every device holds until exit and that all calls on a device share:
  * calls that overlap on the GPU race.  count above MP_NOALLOC_MAX_COUNT is refused with
  * MP_EINVAL.  The first call on a device looks up the array's device address; make that

@@ -14,24 +14,113 @@
 // to right: square, then double when the bit is 1 (base 2 needs no multiplier table).
 #include "mp_common.cuh"
 
+// t[0..K+1] += a[0..K-1] * b: the low halves of the products in one carry chain, then the
+// high halves one word up in a second; each chain is one asm block, so that nothing between
+// its instructions can touch the carry flag.  The multiply-adds run on the multiply pipe.
+template <int K>
+__device__ __forceinline__ void mac_row(u32 (&t)[K + 2], const u32 (&a)[K], u32 b);
+
+template <>
+__device__ __forceinline__ void mac_row<3>(u32 (&t)[5], const u32 (&a)[3], u32 b)
+{
+    asm("mad.lo.cc.u32  %0, %5, %8, %0;\n\t"
+        "madc.lo.cc.u32 %1, %6, %8, %1;\n\t"
+        "madc.lo.cc.u32 %2, %7, %8, %2;\n\t"
+        "addc.cc.u32    %3, %3, 0;\n\t"
+        "addc.u32       %4, %4, 0;\n\t"
+        "mad.hi.cc.u32  %1, %5, %8, %1;\n\t"
+        "madc.hi.cc.u32 %2, %6, %8, %2;\n\t"
+        "madc.hi.cc.u32 %3, %7, %8, %3;\n\t"
+        "addc.u32       %4, %4, 0;"
+        : "+r"(t[0]), "+r"(t[1]), "+r"(t[2]), "+r"(t[3]), "+r"(t[4])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(b));
+}
+
+template <>
+__device__ __forceinline__ void mac_row<4>(u32 (&t)[6], const u32 (&a)[4], u32 b)
+{
+    asm("mad.lo.cc.u32  %0, %6, %10, %0;\n\t"
+        "madc.lo.cc.u32 %1, %7, %10, %1;\n\t"
+        "madc.lo.cc.u32 %2, %8, %10, %2;\n\t"
+        "madc.lo.cc.u32 %3, %9, %10, %3;\n\t"
+        "addc.cc.u32    %4, %4, 0;\n\t"
+        "addc.u32       %5, %5, 0;\n\t"
+        "mad.hi.cc.u32  %1, %6, %10, %1;\n\t"
+        "madc.hi.cc.u32 %2, %7, %10, %2;\n\t"
+        "madc.hi.cc.u32 %3, %8, %10, %3;\n\t"
+        "madc.hi.cc.u32 %4, %9, %10, %4;\n\t"
+        "addc.u32       %5, %5, 0;"
+        : "+r"(t[0]), "+r"(t[1]), "+r"(t[2]), "+r"(t[3]), "+r"(t[4]), "+r"(t[5])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b));
+}
+
+// t - n with the borrow out in one chain: returns 0 when t >= n, all ones otherwise
+template <int K>
+__device__ __forceinline__ u32 sub_n(u32 (&d)[K], const u32 (&t)[K], const u32 (&n)[K]);
+
+template <>
+__device__ __forceinline__ u32 sub_n<3>(u32 (&d)[3], const u32 (&t)[3], const u32 (&n)[3])
+{
+    u32 bw;
+    asm("sub.cc.u32  %0, %4, %7;\n\t"
+        "subc.cc.u32 %1, %5, %8;\n\t"
+        "subc.cc.u32 %2, %6, %9;\n\t"
+        "subc.u32    %3, 0, 0;"
+        : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(bw)
+        : "r"(t[0]), "r"(t[1]), "r"(t[2]), "r"(n[0]), "r"(n[1]), "r"(n[2]));
+    return bw;
+}
+
+template <>
+__device__ __forceinline__ u32 sub_n<4>(u32 (&d)[4], const u32 (&t)[4], const u32 (&n)[4])
+{
+    u32 bw;
+    asm("sub.cc.u32  %0, %5, %9;\n\t"
+        "subc.cc.u32 %1, %6, %10;\n\t"
+        "subc.cc.u32 %2, %7, %11;\n\t"
+        "subc.cc.u32 %3, %8, %12;\n\t"
+        "subc.u32    %4, 0, 0;"
+        : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3]), "=r"(bw)
+        : "r"(t[0]), "r"(t[1]), "r"(t[2]), "r"(t[3]), "r"(n[0]), "r"(n[1]), "r"(n[2]), "r"(n[3]));
+    return bw;
+}
+
 template <int K>
 __device__ __forceinline__ void cond_sub(u32 (&t)[K], u32 top, const u32 (&n)[K])
 {
     // t (with carry word `top`) < 2N: subtract N once if t >= N
     u32 d[K];
-    u64 borrow = 0;
-#pragma unroll
-    for (int j = 0; j < K; j++) {
-        const u64 s = (u64)t[j] - n[j] - borrow;
-        d[j] = (u32)s;
-        borrow = (s >> 63) & 1;
-    }
-    const bool ge = top || !borrow;
+    const u32 bw = sub_n<K>(d, t, n);
+    const bool ge = top || !bw;
 #pragma unroll
     for (int j = 0; j < K; j++) t[j] = ge ? d[j] : t[j];
 }
 
-// r = a * b / R mod N (a, b < N), CIOS with 32-bit limbs
+// r = a * b / R mod N, CIOS with 32-bit limbs: per word b[i], t += a b[i], then t += m N with
+// m = t[0] (-N^-1) mod 2^32, which clears t[0], and t shifts down a word.  With a, b < 2N and
+// 4N < R the result (ab + mN) / R is below N (4N / R + 1) < 2N, so values stay in [0, 2N)
+// without a subtraction (lazy reduction); only the value that leaves the loop is reduced.
+template <int K>
+__device__ __forceinline__ void mmul_lazy(u32 (&r)[K], const u32 (&a)[K], const u32 (&b)[K], const u32 (&n)[K],
+                                          u32 np)
+{
+    u32 t[K + 2];
+#pragma unroll
+    for (int j = 0; j < K + 2; j++) t[j] = 0;
+#pragma unroll
+    for (int i = 0; i < K; i++) {
+        mac_row<K>(t, a, b[i]);
+        const u32 m = t[0] * np;
+        mac_row<K>(t, n, m);
+#pragma unroll
+        for (int j = 0; j < K + 1; j++) t[j] = t[j + 1];
+        t[K + 1] = 0;
+    }
+#pragma unroll
+    for (int j = 0; j < K; j++) r[j] = t[j];                 // t < 2N < R: t[K] = 0
+}
+
+// the same, reduced to [0, N)
 template <int K>
 __device__ __forceinline__ void mmul(u32 (&r)[K], const u32 (&a)[K], const u32 (&b)[K], const u32 (&n)[K], u32 np)
 {
@@ -40,28 +129,12 @@ __device__ __forceinline__ void mmul(u32 (&r)[K], const u32 (&a)[K], const u32 (
     for (int j = 0; j < K + 2; j++) t[j] = 0;
 #pragma unroll
     for (int i = 0; i < K; i++) {
-        u64 C = 0;
-#pragma unroll
-        for (int j = 0; j < K; j++) {
-            const u64 s = (u64)t[j] + (u64)a[j] * b[i] + C;
-            t[j] = (u32)s;
-            C = s >> 32;
-        }
-        u64 s = (u64)t[K] + C;
-        t[K] = (u32)s;
-        t[K + 1] = (u32)(s >> 32);
+        mac_row<K>(t, a, b[i]);
         const u32 m = t[0] * np;
-        s = (u64)t[0] + (u64)m * n[0];
-        C = s >> 32;
+        mac_row<K>(t, n, m);
 #pragma unroll
-        for (int j = 1; j < K; j++) {
-            s = (u64)t[j] + (u64)m * n[j] + C;
-            t[j - 1] = (u32)s;
-            C = s >> 32;
-        }
-        s = (u64)t[K] + C;
-        t[K - 1] = (u32)s;
-        t[K] = t[K + 1] + (u32)(s >> 32);
+        for (int j = 0; j < K + 1; j++) t[j] = t[j + 1];
+        t[K + 1] = 0;
     }
     u32 o[K];
 #pragma unroll
@@ -71,7 +144,7 @@ __device__ __forceinline__ void mmul(u32 (&r)[K], const u32 (&a)[K], const u32 (
     for (int j = 0; j < K; j++) r[j] = o[j];
 }
 
-// x = 2x mod N (x < N, 2N < R)
+// x = 2x, reduced below m (x < m, 2m <= R): m = N keeps [0, N), m = 2N keeps [0, 2N)
 template <int K>
 __device__ __forceinline__ void mdbl(u32 (&x)[K], const u32 (&n)[K])
 {
@@ -106,19 +179,25 @@ __device__ __forceinline__ FermOut fermat_one(u64 p)
 #pragma unroll
     for (int j = 0; j < K; j++) x[j] = (topbit >> 5) == j ? (1u << (topbit & 31)) : 0u;
     for (int i = topbit; i < 32 * K; i++) mdbl<K>(x, n);
-    // left-to-right binary exponentiation of 2 to e = p - 1; leading zero bits keep x = 1
+    // left-to-right binary exponentiation of 2 to e = p - 1 on representatives in [0, 2N)
+    // (lazy reduction; 4N < R for both limb counts); leading zero bits keep x = 1
+    u32 n2[K];
+    n2[0] = n[0] << 1;
+#pragma unroll
+    for (int j = 1; j < K; j++) n2[j] = (n[j] << 1) | (n[j - 1] >> 31);
     const u64 e = p - 1;
     for (int b = 63 - __clzll((long long)e); b >= 0; b--) {
-        mmul<K>(x, x, x, n, np);
+        mmul_lazy<K>(x, x, x, n, np);
         u32 y[K];
 #pragma unroll
         for (int j = 0; j < K; j++) y[j] = x[j];
-        mdbl<K>(y, n);
+        mdbl<K>(y, n2);
         const bool bit = (e >> b) & 1;
 #pragma unroll
         for (int j = 0; j < K; j++) x[j] = bit ? y[j] : x[j];
     }
-    // leave Montgomery form: multiply by 1
+    // leave Montgomery form: multiply by 1; with x < 2N the product (x + mN) / R is at most N,
+    // and mmul's subtraction brings it to [0, N)
     u32 one[K];
 #pragma unroll
     for (int j = 0; j < K; j++) one[j] = j == 0 ? 1u : 0u;
@@ -172,28 +251,42 @@ __device__ __forceinline__ void fp_join(FermPart &L, const FermPart &R)
     L.cks += R.cks; L.near += R.near; L.flt += R.flt; L.tests += R.tests;
 }
 
-__global__ void __launch_bounds__(256) fermat_stats_kernel(const u64 *__restrict__ P, const u64 *__restrict__ Q, u64 count,
-                                                            FermPart *parts, u64 *hits, u64 *nhits)
+#define FS_THREADS 256
+#define FS_PER 8                                           // consecutive entries per thread
+#define FS_TILE (FS_THREADS * FS_PER)                      // entries per CTA
+
+// one CTA per FS_TILE entries: the tile's primes and quotients are staged in shared memory
+// with coalesced loads, each thread folds its FS_PER consecutive entries in order (the ordered
+// hash by Horner's rule), then the threads join in order
+__global__ void __launch_bounds__(FS_THREADS) fermat_stats_kernel(const u64 *__restrict__ P, const u64 *__restrict__ Q,
+                                                                  u64 count, FermPart *parts, u64 *hits, u64 *nhits)
 {
-    __shared__ FermPart s_w[8];
-    const u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    __shared__ FermPart s_w[FS_THREADS / 32];
+    // entry k at k + k / FS_PER: a thread's FS_PER entries are 9 words apart from the next
+    // thread's, which keeps the reads nearly free of bank conflicts
+    __shared__ u64 sp[FS_TILE + FS_TILE / FS_PER], sq[FS_TILE + FS_TILE / FS_PER];
+    const u64 t0 = (u64)blockIdx.x * FS_TILE;
+    for (u32 k = threadIdx.x; k < FS_TILE; k += FS_THREADS) {
+        const bool in = t0 + k < count;
+        sp[k + k / FS_PER] = in ? __ldcs(P + t0 + k) : 0;
+        sq[k + k / FS_PER] = in ? __ldcs(Q + t0 + k) : 0;
+    }
+    __syncthreads();
     FermPart f = {0, 0, 0, 0, 0, 0};
-    if (i < count) {
-        const u64 p = P[i], q = Q[i];
-        if (p >= 3) {
-            f.tests = 1;
-            if (q >= p) f.flt = 1;
-            else {
-                f.cks = mp_mix64(q ^ (p * MP_GOLD));
-                const u64 A = q <= p / 2 ? q : p - q;
-                f.near = A <= (p - 1) / 1000;              // 1000 A < p
-                f.h = mp_mix64(p ^ mp_mix64(q));
-                f.len = 1;
-                if (q == 0) {
-                    const u64 k = atomicAdd((unsigned long long *)nhits, 1ull);
-                    if (k < 16) hits[k] = p;
-                }
-            }
+#pragma unroll
+    for (int u = 0; u < FS_PER; u++) {
+        const u64 p = sp[threadIdx.x * (FS_PER + 1) + u], q = sq[threadIdx.x * (FS_PER + 1) + u];
+        if (p < 3) continue;                               // 2 is not tested (and padding)
+        f.tests++;
+        if (q >= p) { f.flt++; continue; }
+        f.cks += mp_mix64(q ^ (p * MP_GOLD));
+        const u64 A = q <= p / 2 ? q : p - q;
+        f.near += A <= (p - 1) / 1000;                     // 1000 A < p
+        f.h = f.h * MP_FNV_PRIME + mp_mix64(p ^ mp_mix64(q));
+        f.len++;
+        if (q == 0) {
+            const u64 k = atomicAdd((unsigned long long *)nhits, 1ull);
+            if (k < 16) hits[k] = p;
         }
     }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -212,7 +305,7 @@ __global__ void __launch_bounds__(256) fermat_stats_kernel(const u64 *__restrict
     __syncthreads();
     if (threadIdx.x == 0) {
         FermPart b = s_w[0];
-        for (int w = 1; w < (int)(blockDim.x >> 5); w++) fp_join(b, s_w[w]);
+        for (int w = 1; w < FS_THREADS / 32; w++) fp_join(b, s_w[w]);
         parts[blockIdx.x] = b;
     }
 }
@@ -262,7 +355,7 @@ int mp_fermat_run(mp_handle *h, const u64 *d_p, u64 count, u64 *d_q, cudaStream_
 
 int mp_fermat_reduce(mp_handle *h, const u64 *d_p, const u64 *d_q, u64 count, mp_wief_stats *d_stats, cudaStream_t st)
 {
-    const u64 nb = count ? (count + 255) / 256 : 1;
+    const u64 nb = count ? (count + FS_TILE - 1) / FS_TILE : 1;
     MP_CUDA(h, h->ferm_part.ensure((size_t)nb * sizeof(FermPart) + 256));
     FermPart *parts = h->ferm_part.as<FermPart>();
     u64 *hits = (u64 *)((char *)h->ferm_part.p + nb * sizeof(FermPart));
@@ -270,7 +363,7 @@ int mp_fermat_reduce(mp_handle *h, const u64 *d_p, const u64 *d_q, u64 count, mp
     MP_CUDA(h, cudaMemsetAsync(hits, 0, 17 * 8, st));
     if (count) {
         ProfScope ps(h, PROF_FERMAT_STATS, st);
-        fermat_stats_kernel<<<(unsigned)nb, 256, 0, st>>>(d_p, d_q, count, parts, hits, nhits);
+        fermat_stats_kernel<<<(unsigned)nb, FS_THREADS, 0, st>>>(d_p, d_q, count, parts, hits, nhits);
         MP_CUDA(h, cudaGetLastError());
     } else {
         MP_CUDA(h, cudaMemsetAsync(parts, 0, sizeof(FermPart), st));
@@ -291,10 +384,10 @@ int mp_fermat_reduce(mp_handle *h, const u64 *d_p, const u64 *d_q, u64 count, mp
 // ---------------------------------------------------------------------------------------
 
 #define NOALLOC_MAX_COUNT (1u << 24)                       // primes per call
-#define NOALLOC_PARTS (NOALLOC_MAX_COUNT / 256)           // one partial per 256-thread CTA
+#define NOALLOC_PARTS (NOALLOC_MAX_COUNT / FS_TILE)       // one partial per CTA
 
 struct NoallocScratch {
-    FermPart parts[NOALLOC_PARTS];                          // 3 MB
+    FermPart parts[NOALLOC_PARTS];                          // 384 KB
     u64 hits[16];
     u64 nhits;
 };
@@ -346,8 +439,8 @@ extern "C" int mp_wieferich_stats_noalloc(const uint64_t *d_p, const uint64_t *d
     cudaStream_t st = (cudaStream_t)stream;
     // the hit list carries over from the previous call: it must start at zero
     noalloc_clear_kernel<<<1, 32, 0, st>>>(s);
-    const u64 nb = count ? (count + 255) / 256 : 0;
-    if (count) fermat_stats_kernel<<<(unsigned)nb, 256, 0, st>>>(d_p, d_q, count, s->parts, s->hits, &s->nhits);
+    const u64 nb = count ? (count + FS_TILE - 1) / FS_TILE : 0;
+    if (count) fermat_stats_kernel<<<(unsigned)nb, FS_THREADS, 0, st>>>(d_p, d_q, count, s->parts, s->hits, &s->nhits);
     else {
         // no input: one empty partial
         if (cudaMemsetAsync(s->parts, 0, sizeof(FermPart), st) != cudaSuccess) return MP_ECUDA;
