@@ -231,8 +231,11 @@ int mp_probe_peaks(mp_handle *h, double *smem_atomic_conflict_free, double *smem
  * Requests of two kinds: range queries [lo, hi) -> pi, max gap (+ start), twins; and
  * primality batches of up to 65536 candidates -> verdict bits.  Requests are admitted
  * while device memory (a budget) and in-flight slots allow; admitted work is cut into
- * tiles and candidate slices that share the device with other requests' work.  Each
- * result is identical to the same request run alone.
+ * tiles and candidate slices that share the device with other requests' work.  A long
+ * range runs a chunk at a time and goes back to the end of the queue between chunks, so
+ * short requests are not held up behind it.  Every worker's scratch is sized at open for
+ * its largest turn, so that no buffer grows (and no cudaFree synchronises the device) while
+ * requests run.  Each result is identical to the same request run alone.
  */
 typedef struct mp_server mp_server;
 
@@ -241,6 +244,9 @@ typedef struct {
     uint32_t max_inflight;  /* requests admitted at once (0 = 256) */
     uint32_t streams;       /* device streams that overlap batches (0 = 4) */
     uint64_t prime_limit;   /* resident sieving primes up to this bound (0 = 2^30: heights to ~1.15e18) */
+    uint64_t chunk;         /* a range request runs at least this many integers at a time (and at
+                               least 64 per sieving prime up to its sqrt(hi)), then yields to the
+                               queue (processor sharing); 0 = 2^32 */
 } mp_serve_opts;
 
 typedef struct {

@@ -55,7 +55,7 @@ STATS_DTYPE = np.dtype([(n, np.uint64) for n in STATS_FIELDS])
 
 class ServeOpts(C.Structure):
     _fields_ = [("mem_budget", C.c_uint64), ("max_inflight", C.c_uint32), ("streams", C.c_uint32),
-                ("prime_limit", C.c_uint64)]
+                ("prime_limit", C.c_uint64), ("chunk", C.c_uint64)]
 
 
 class ServeResult(C.Structure):
@@ -293,10 +293,10 @@ class Engine:
 class Server:
     """Continuous-batching request server on an Engine (mp_serve_*)."""
 
-    def __init__(self, engine, streams=4, max_inflight=256, mem_budget=0, prime_limit=0):
+    def __init__(self, engine, streams=4, max_inflight=256, mem_budget=0, prime_limit=0, chunk=0):
         self.e = engine
         self._s = C.c_void_p()
-        o = ServeOpts(mem_budget, max_inflight, streams, prime_limit)
+        o = ServeOpts(mem_budget, max_inflight, streams, prime_limit, chunk)
         engine._check(lib().mp_serve_open(engine.handle, C.byref(o), C.byref(self._s)))
         self._bits = {}
 

@@ -6,14 +6,20 @@
 // the next request when an in-flight slot is free and the request's device-memory estimate
 // fits in what the budget has left (admission by free device memory), so requests that
 // arrive while others are on the GPU are admitted as soon as slots and memory free up.
-//   range request      runs the batched sieve on the worker's stream; K workers overlap on
-//                      the device;
+//   range request      runs the batched sieve on the worker's stream, at most `chunk`
+//                      integers at a time: a longer range goes back to the end of the queue
+//                      after each chunk (processor sharing), so that the short requests
+//                      behind it are not held up for its whole length.  The chunks' results
+//                      join exactly: counts add, and every gap belongs to the chunk of the
+//                      prime that starts it (each chunk sees the primes past its end);
+//                      K workers overlap on the device;
 //   primality request  a worker that picks one takes every primality request waiting at
 //                      that moment (up to a candidate cap) and runs them as ONE persistent
 //                      batched BPSW launch over all their lists (continuous batching).
 // Results are those of the same request run alone: the kernels are the same and every
 // request has its own outputs; only scheduling differs.
 #include "mp_common.cuh"
+#include <algorithm>
 #include <chrono>
 #include <condition_variable>
 #include <deque>
@@ -24,6 +30,8 @@ struct ServeReq {
     u64 id = 0;
     u32 kind = 0;                    // 1 range, 2 primality
     u64 lo = 0, hi = 0;
+    u64 next = 0;                    // range: the first integer not yet sieved
+    u64 chunk = 0;                   // range: integers per turn
     std::vector<u64> cand;
     u8 *out_bits = nullptr;
     u64 mem = 0;
@@ -44,6 +52,7 @@ struct mp_server {
     u64 budget = 0, mem_used = 0;
     u32 max_inflight = 256, inflight = 0;
     u64 prime_limit = 0;
+    u64 chunk = 1ull << 32;          // least integers of a range request per turn
     u64 bpsw_cap = 1ull << 22;       // candidates per merged primality launch
 };
 
@@ -63,19 +72,23 @@ static u64 range_mem(u64 lo, u64 hi)
 
 static u64 bpsw_mem(u64 count) { return count * 8 + count / 8 + 4096; }
 
-static void run_range(mp_handle *w, ServeReq *r)
+// the next chunk of a range request, joined into its result; true when the range is done
+static bool run_range(mp_handle *w, ServeReq *r)
 {
+    const u64 chunk = r->chunk;
     mp_sieve_opts o;
     memset(&o, 0, sizeof o);
     o.mode = MP_MODE_BATCHED;
     mp_range_stats st;
     memset(&st, 0, sizeof st);
-    const int rc = mp_sieve_range(w, r->lo, r->hi, &o, &st, nullptr, nullptr, nullptr);
-    r->res.status = rc;
-    r->res.pi = st.pi;
-    r->res.max_gap = st.max_gap;
-    r->res.gap_start = st.gap_start;
-    r->res.twins = st.twins;
+    const u64 a = r->next, b = r->hi - a > chunk ? a + chunk : r->hi;
+    const int rc = mp_sieve_range(w, a, b, &o, &st, nullptr, nullptr, nullptr);
+    if (rc != MP_OK) { r->res.status = rc; return true; }
+    r->res.pi += st.pi;
+    r->res.twins += st.twins;
+    if (st.max_gap > r->res.max_gap) { r->res.max_gap = st.max_gap; r->res.gap_start = st.gap_start; }
+    r->next = b;
+    return b >= r->hi;
 }
 
 static void run_bpsw(mp_handle *w, std::vector<ServeReq *> &batch)
@@ -130,15 +143,17 @@ static void worker_loop(mp_server *s, mp_handle *w)
             for (ServeReq *r : take) s->mem_used += r->mem;
             s->inflight += (u32)take.size();
         }
-        if (take[0]->kind == 1) run_range(w, take[0]);
+        bool finished = true;
+        if (take[0]->kind == 1) finished = run_range(w, take[0]);
         else run_bpsw(w, take);
         {
             std::lock_guard<std::mutex> lk(s->mu);
             const double t = now_s();
             for (ServeReq *r : take) {
+                s->mem_used -= r->mem;
+                if (!finished) { s->pending.push_back(r); continue; }   // its next turn
                 r->res.done_s = t;
                 r->done = true;
-                s->mem_used -= r->mem;
             }
             s->inflight -= (u32)take.size();
         }
@@ -168,6 +183,7 @@ int mp_serve_open(mp_handle *h, const mp_serve_opts *opts, mp_server **out)
     MP_CUDA(h, cudaMemGetInfo(&fr, &tot));
     s->budget = o.mem_budget ? o.mem_budget : (u64)fr / 2;
     s->max_inflight = o.max_inflight ? o.max_inflight : 256;
+    s->chunk = o.chunk ? o.chunk : (1ull << 32);
     const u32 k = o.streams ? o.streams : 4;
     for (u32 i = 0; i < k; i++) {
         mp_handle *w = nullptr;
@@ -183,6 +199,32 @@ int mp_serve_open(mp_handle *h, const mp_serve_opts *opts, mp_server **out)
         w->no_graphs = true;
         w->tune = h->tune;
         s->workers.push_back(w);
+    }
+    // Size every worker's scratch for its largest turn now: a buffer that grows later frees
+    // the old one, and cudaFree synchronises the whole device, which stalls every worker.
+    // The largest turn is the longest chunk at the top height the table serves; the largest
+    // primality launch is one merged batch.
+    {
+        const u64 pl = std::min<u64>(s->prime_limit, 0xffffffffull);
+        const u64 top = std::min<u64>(MP_HI_MAX, pl * pl - MP_TAIL);
+        const u64 len = std::min<u64>(std::max<u64>(s->chunk, 64 * h->tab->count_le(pl)), top / 2);
+        std::vector<u64> zeros(s->bpsw_cap, 0);
+        const uint64_t *lists[1] = {zeros.data()};
+        const uint32_t lens[1] = {(uint32_t)zeros.size()};
+        std::vector<u8> bits(zeros.size() / 8 + 8);
+        uint8_t *outs[1] = {bits.data()};
+        mp_sieve_opts wo;
+        memset(&wo, 0, sizeof wo);
+        for (mp_handle *w : s->workers) {
+            mp_range_stats st;
+            int rc = mp_sieve_range(w, top - len, top, &wo, &st, nullptr, nullptr, nullptr);
+            if (rc == MP_OK) rc = mp_bpsw_batches(w, lists, lens, 1, outs);
+            if (rc != MP_OK) {
+                const int e = mp_set_error(h, rc, "serving worker warm-up failed: %s", w->err);
+                mp_serve_close(s);
+                return e;
+            }
+        }
     }
     for (mp_handle *w : s->workers) s->threads.emplace_back(worker_loop, s, w);
     h->servers_open++;
@@ -214,7 +256,12 @@ int mp_serve_submit_range(mp_server *s, uint64_t lo, uint64_t hi, uint64_t *req_
     r->kind = 1;
     r->lo = lo;
     r->hi = hi;
-    r->mem = range_mem(lo, hi);
+    r->next = lo;
+    // every turn sets up the large sieving primes of the range again (about the work of 15
+    // integers each), so a turn covers at least 64 integers per sieving prime up to sqrt(hi)
+    const u64 np = s->main->tab->count_le(mp_isqrt64(hi + MP_TAIL - 1));
+    r->chunk = std::max<u64>(s->chunk, 64 * np);
+    r->mem = range_mem(lo, hi - lo > r->chunk ? lo + r->chunk : hi);   // one chunk in flight
     r->res.kind = 1;
     return submit(s, r, req_id);
 }

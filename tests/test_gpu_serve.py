@@ -48,6 +48,34 @@ def test_mixed_stream_equals_alone(engine):
             assert np.array_equal(g["verdicts"], engine.bpsw(r[1]))
 
 
+def test_chunked_ranges_equal_alone(engine):
+    """Ranges much longer than the serving chunk run in turns, interleaved with other requests,
+    and join to the result of the whole range run alone."""
+    import mathpub_b200 as mp
+    reqs = _stream(29, 24, 24)
+    with mp.Server(engine, streams=3, chunk=1 << 22) as srv:
+        ids = [srv.submit_range(r[1], r[2]) if r[0] == "range" else srv.submit_bpsw(r[1]) for r in reqs]
+        got = []
+        for rid in ids:
+            res = None
+            for _ in range(600):
+                res = srv.poll(rid, wait_ms=500)
+                if res is not None:
+                    break
+            assert res is not None and res["status"] == 0
+            got.append(res)
+    nchunked = 0
+    for r, g in zip(reqs, got):
+        if r[0] == "range":
+            nchunked += r[2] - r[1] > 1 << 22
+            alone = engine.sieve_range(r[1], r[2])
+            for k in ("pi", "max_gap", "gap_start", "twins"):
+                assert g[k] == alone[k], (r, k)
+        else:
+            assert np.array_equal(g["verdicts"], engine.bpsw(r[1]))
+    assert nchunked >= 5
+
+
 def test_out_of_table_range_is_refused(engine):
     import mathpub_b200 as mp
     fresh = mp.Engine(0)             # its table is only as large as the server asks
