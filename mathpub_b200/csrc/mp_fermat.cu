@@ -14,43 +14,40 @@
 // to right: square, then double when the bit is 1 (base 2 needs no multiplier table).
 #include "mp_common.cuh"
 
-// t[0..K+1] += a[0..K-1] * b: the low halves of the products in one carry chain, then the
-// high halves one word up in a second; each chain is one asm block, so that nothing between
-// its instructions can touch the carry flag.  The multiply-adds run on the multiply pipe.
+// t[0..K] += a[0..K-1] * b: the low halves of the products in one carry chain, then the high
+// halves one word up in a second; each chain is one asm block, so that nothing between its
+// instructions can touch the carry flag.  The multiply-adds run on the multiply pipe.  The
+// callers keep t below 2^(32 (K + 1)), so nothing carries out of t[K] (see mmul_lazy).
 template <int K>
-__device__ __forceinline__ void mac_row(u32 (&t)[K + 2], const u32 (&a)[K], u32 b);
+__device__ __forceinline__ void mac_row(u32 (&t)[K + 1], const u32 (&a)[K], u32 b);
 
 template <>
-__device__ __forceinline__ void mac_row<3>(u32 (&t)[5], const u32 (&a)[3], u32 b)
+__device__ __forceinline__ void mac_row<3>(u32 (&t)[4], const u32 (&a)[3], u32 b)
 {
-    asm("mad.lo.cc.u32  %0, %5, %8, %0;\n\t"
-        "madc.lo.cc.u32 %1, %6, %8, %1;\n\t"
-        "madc.lo.cc.u32 %2, %7, %8, %2;\n\t"
-        "addc.cc.u32    %3, %3, 0;\n\t"
-        "addc.u32       %4, %4, 0;\n\t"
-        "mad.hi.cc.u32  %1, %5, %8, %1;\n\t"
-        "madc.hi.cc.u32 %2, %6, %8, %2;\n\t"
-        "madc.hi.cc.u32 %3, %7, %8, %3;\n\t"
-        "addc.u32       %4, %4, 0;"
-        : "+r"(t[0]), "+r"(t[1]), "+r"(t[2]), "+r"(t[3]), "+r"(t[4])
+    asm("mad.lo.cc.u32  %0, %4, %7, %0;\n\t"
+        "madc.lo.cc.u32 %1, %5, %7, %1;\n\t"
+        "madc.lo.cc.u32 %2, %6, %7, %2;\n\t"
+        "addc.u32       %3, %3, 0;\n\t"
+        "mad.hi.cc.u32  %1, %4, %7, %1;\n\t"
+        "madc.hi.cc.u32 %2, %5, %7, %2;\n\t"
+        "madc.hi.u32    %3, %6, %7, %3;"
+        : "+r"(t[0]), "+r"(t[1]), "+r"(t[2]), "+r"(t[3])
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(b));
 }
 
 template <>
-__device__ __forceinline__ void mac_row<4>(u32 (&t)[6], const u32 (&a)[4], u32 b)
+__device__ __forceinline__ void mac_row<4>(u32 (&t)[5], const u32 (&a)[4], u32 b)
 {
-    asm("mad.lo.cc.u32  %0, %6, %10, %0;\n\t"
-        "madc.lo.cc.u32 %1, %7, %10, %1;\n\t"
-        "madc.lo.cc.u32 %2, %8, %10, %2;\n\t"
-        "madc.lo.cc.u32 %3, %9, %10, %3;\n\t"
-        "addc.cc.u32    %4, %4, 0;\n\t"
-        "addc.u32       %5, %5, 0;\n\t"
-        "mad.hi.cc.u32  %1, %6, %10, %1;\n\t"
-        "madc.hi.cc.u32 %2, %7, %10, %2;\n\t"
-        "madc.hi.cc.u32 %3, %8, %10, %3;\n\t"
-        "madc.hi.cc.u32 %4, %9, %10, %4;\n\t"
-        "addc.u32       %5, %5, 0;"
-        : "+r"(t[0]), "+r"(t[1]), "+r"(t[2]), "+r"(t[3]), "+r"(t[4]), "+r"(t[5])
+    asm("mad.lo.cc.u32  %0, %5, %9, %0;\n\t"
+        "madc.lo.cc.u32 %1, %6, %9, %1;\n\t"
+        "madc.lo.cc.u32 %2, %7, %9, %2;\n\t"
+        "madc.lo.cc.u32 %3, %8, %9, %3;\n\t"
+        "addc.u32       %4, %4, 0;\n\t"
+        "mad.hi.cc.u32  %1, %5, %9, %1;\n\t"
+        "madc.hi.cc.u32 %2, %6, %9, %2;\n\t"
+        "madc.hi.cc.u32 %3, %7, %9, %3;\n\t"
+        "madc.hi.u32    %4, %8, %9, %4;"
+        : "+r"(t[0]), "+r"(t[1]), "+r"(t[2]), "+r"(t[3]), "+r"(t[4])
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b));
 }
 
@@ -100,48 +97,33 @@ __device__ __forceinline__ void cond_sub(u32 (&t)[K], u32 top, const u32 (&n)[K]
 // m = t[0] (-N^-1) mod 2^32, which clears t[0], and t shifts down a word.  With a, b < 2N and
 // 4N < R the result (ab + mN) / R is below N (4N / R + 1) < 2N, so values stay in [0, 2N)
 // without a subtraction (lazy reduction); only the value that leaves the loop is reduced.
+// Bounds: before a row pair t < 3N (K words), after it t < 3N (1 + 2^32) < 2^(32 (K + 1)).
 template <int K>
 __device__ __forceinline__ void mmul_lazy(u32 (&r)[K], const u32 (&a)[K], const u32 (&b)[K], const u32 (&n)[K],
                                           u32 np)
 {
-    u32 t[K + 2];
+    u32 t[K + 1];
 #pragma unroll
-    for (int j = 0; j < K + 2; j++) t[j] = 0;
+    for (int j = 0; j < K + 1; j++) t[j] = 0;
 #pragma unroll
     for (int i = 0; i < K; i++) {
         mac_row<K>(t, a, b[i]);
         const u32 m = t[0] * np;
         mac_row<K>(t, n, m);
 #pragma unroll
-        for (int j = 0; j < K + 1; j++) t[j] = t[j + 1];
-        t[K + 1] = 0;
+        for (int j = 0; j < K; j++) t[j] = t[j + 1];
+        t[K] = 0;
     }
 #pragma unroll
-    for (int j = 0; j < K; j++) r[j] = t[j];                 // t < 2N < R: t[K] = 0
+    for (int j = 0; j < K; j++) r[j] = t[j];
 }
 
-// the same, reduced to [0, N)
+// the same, reduced to [0, N) (for a product below 2N)
 template <int K>
 __device__ __forceinline__ void mmul(u32 (&r)[K], const u32 (&a)[K], const u32 (&b)[K], const u32 (&n)[K], u32 np)
 {
-    u32 t[K + 2];
-#pragma unroll
-    for (int j = 0; j < K + 2; j++) t[j] = 0;
-#pragma unroll
-    for (int i = 0; i < K; i++) {
-        mac_row<K>(t, a, b[i]);
-        const u32 m = t[0] * np;
-        mac_row<K>(t, n, m);
-#pragma unroll
-        for (int j = 0; j < K + 1; j++) t[j] = t[j + 1];
-        t[K + 1] = 0;
-    }
-    u32 o[K];
-#pragma unroll
-    for (int j = 0; j < K; j++) o[j] = t[j];
-    cond_sub<K>(o, t[K], n);
-#pragma unroll
-    for (int j = 0; j < K; j++) r[j] = o[j];
+    mmul_lazy<K>(r, a, b, n, np);
+    cond_sub<K>(r, 0u, n);
 }
 
 // x = 2x, reduced below m (x < m, 2m <= R): m = N keeps [0, N), m = 2N keeps [0, 2N)
