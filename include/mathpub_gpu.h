@@ -135,14 +135,26 @@ int mp_primes_range(mp_handle *h, uint64_t lo, uint64_t hi, uint64_t *primes, si
  * histogram of A252768/a252768.c (its chunk totals).  hi <= 2^64 - 2^18 - 2^17. */
 #define MP_GAP_BINS 1024
 #define MP_RUN_MAX 64
+#define MP_CHAIN_MAX 32
 typedef struct {
     uint64_t gap_hist[MP_GAP_BINS];
     uint64_t run_hist[MP_RUN_MAX];
     uint64_t run_first[MP_RUN_MAX];
     uint64_t unsettled;
+    /* chain_hist[L]: primes p in [lo, hi) that head a chain of exactly L consecutive primes
+       with gaps 2, 4, 6, ..., 2(L - 1) (A016045; the members are p + m(m + 1), m < L); the
+       last bin holds L >= MP_CHAIN_MAX - 1 */
+    uint64_t chain_hist[MP_CHAIN_MAX];
 } mp_gap_stats;
 
 int mp_gap_stats_range(mp_handle *h, uint64_t lo, uint64_t hi, mp_gap_stats *out);
+
+/* the heads p in [lo, hi) of chains of at least min_len (>= 2) primes with gaps 2, 4, 6, ...,
+ * in increasing order, with their lengths (capped at MP_CHAIN_MAX - 1), into caller arrays of
+ * cap entries; *count = the number of heads (only min(count, cap) are written).  Replaces the
+ * chain walk of gapchain/gapchain_ps.c:336-366 (its default --gaps inc) over the same range. */
+int mp_gap_chains(mp_handle *h, uint64_t lo, uint64_t hi, uint32_t min_len, uint64_t *heads, uint32_t *lens,
+                  size_t cap, size_t *count);
 
 /* ---- BPSW ----
  * verdict bit i (bit i & 7 of byte i >> 3) = 1 iff n[i] is prime.  For n < 2^64 this is

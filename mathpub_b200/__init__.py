@@ -64,17 +64,18 @@ class ServeResult(C.Structure):
                 ("submit_s", C.c_double), ("done_s", C.c_double)]
 
 
-GAP_BINS, RUN_MAX = 1024, 64
+GAP_BINS, RUN_MAX, CHAIN_MAX = 1024, 64, 32
 
 
 class GapStats(C.Structure):
     _fields_ = [("gap_hist", C.c_uint64 * GAP_BINS), ("run_hist", C.c_uint64 * RUN_MAX),
-                ("run_first", C.c_uint64 * RUN_MAX), ("unsettled", C.c_uint64)]
+                ("run_first", C.c_uint64 * RUN_MAX), ("unsettled", C.c_uint64), ("chain_hist", C.c_uint64 * CHAIN_MAX)]
 
     def as_dict(self):
         return {"gap_hist": np.ctypeslib.as_array(self.gap_hist).copy(),
                 "run_hist": np.ctypeslib.as_array(self.run_hist).copy(),
-                "run_first": np.ctypeslib.as_array(self.run_first).copy(), "unsettled": int(self.unsettled)}
+                "run_first": np.ctypeslib.as_array(self.run_first).copy(), "unsettled": int(self.unsettled),
+                "chain_hist": np.ctypeslib.as_array(self.chain_hist).copy()}
 
 
 class MathpubError(RuntimeError):
@@ -115,6 +116,7 @@ def lib():
             "mp_wieferich_range": ([vp, u64, u64, vp], C.c_int),
             "mp_wieferich_stats_noalloc": ([vp, vp, u64, vp, vp], C.c_int),
             "mp_gap_stats_range": ([vp, u64, u64, vp], C.c_int),
+            "mp_gap_chains": ([vp, u64, u64, u32, vp, vp, C.c_size_t, C.POINTER(C.c_size_t)], C.c_int),
             "mp_autotune": ([vp, u64, C.c_char_p, C.c_size_t], C.c_int),
             "mp_profile_enable": ([vp, C.c_int], C.c_int),
             "mp_profile_read": ([vp, vp, vp, C.c_int], C.c_int),
@@ -260,6 +262,16 @@ class Engine:
         g = GapStats()
         self._check(lib().mp_gap_stats_range(self._h, lo, hi, C.byref(g)))
         return g.as_dict()
+
+    def gap_chains(self, lo, hi, min_len):
+        """Heads p in [lo, hi) of chains of at least min_len primes with gaps 2, 4, 6, ... and the
+        chain lengths (mp_gap_chains), in increasing order."""
+        n = C.c_size_t()
+        self._check(lib().mp_gap_chains(self._h, lo, hi, min_len, None, None, 0, C.byref(n)))
+        heads = np.zeros(max(1, n.value), dtype=np.uint64)
+        lens = np.zeros(max(1, n.value), dtype=np.uint32)
+        self._check(lib().mp_gap_chains(self._h, lo, hi, min_len, _p(heads), _p(lens), n.value, C.byref(n)))
+        return heads[:n.value], lens[:n.value]
 
     def wieferich_range(self, lo, hi):
         out = WiefStats()

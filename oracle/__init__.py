@@ -203,7 +203,7 @@ def mix64(z):
     return int(o().or_mix64(z))
 
 
-GAP_BINS, RUN_MAX, GAP_LOOK = 1024, 64, 1 << 16
+GAP_BINS, RUN_MAX, CHAIN_MAX, GAP_LOOK = 1024, 64, 32, 1 << 16
 
 
 def gap_stats(lo, hi, nthreads=None):
@@ -240,4 +240,35 @@ def gap_stats(lo, hi, nthreads=None):
     for l in range(1, RUN_MAX):                       # P is increasing: the first index is the smallest p
         if run_hist[l]:
             run_first[l] = P[int(np.argmax(Lc == l))]
-    return {"gap_hist": hist, "run_hist": run_hist, "run_first": run_first, "unsettled": int(unsettled)}
+    cl = chain_lengths(g, len(idx))
+    chain_hist = np.bincount(np.minimum(cl, CHAIN_MAX - 1), minlength=CHAIN_MAX).astype(np.uint64)
+    return {"gap_hist": hist, "run_hist": run_hist, "run_first": run_first, "unsettled": int(unsettled),
+            "chain_hist": chain_hist}
+
+
+def chain_lengths(g, n):
+    """For the first n primes of a list with gaps g: the number of primes in the chain that each
+    heads, the m-th gap being 2m (gapchain/gapchain_ps.c:336-342: len = 1 + the gaps 2, 4, 6, ...
+    that follow p), up to CHAIN_MAX - 1 gaps."""
+    cl = np.ones(n, dtype=np.int64)
+    alive = np.ones(n, dtype=bool)
+    for m in range(1, CHAIN_MAX):
+        j = np.arange(n) + (m - 1)
+        ok = j < len(g)
+        step = np.zeros(n, dtype=bool)
+        step[ok] = g[j[ok]] == 2 * m
+        alive &= step
+        if not alive.any():
+            break
+        cl += alive
+    return cl
+
+
+def gap_chains(lo, hi, min_len, nthreads=None):
+    """Heads p in [lo, hi) of chains of at least min_len primes with gaps 2, 4, 6, ..., and the
+    chain lengths (capped at CHAIN_MAX - 1), in increasing order."""
+    p = primes_range(lo, hi + GAP_LOOK, nthreads).astype(np.int64)
+    n_in = int(np.searchsorted(p, hi))
+    cl = chain_lengths(np.diff(p), n_in)
+    sel = cl >= min_len
+    return p[:n_in][sel].astype(np.uint64), np.minimum(cl[sel], CHAIN_MAX - 1).astype(np.uint32)

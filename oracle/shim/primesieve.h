@@ -22,6 +22,9 @@ typedef struct {
     uint64_t *primes;
     size_t cap;
     int is_error;
+    uint64_t *pbuf;        /* backward buffer of prev_prime: pbuf[0..pi) are still to come */
+    size_t pi, pcap;
+    uint64_t prev_hi;      /* the primes below it are not buffered yet */
 } primesieve_iterator;
 
 void primesieve_init(primesieve_iterator *it);
@@ -29,6 +32,7 @@ void primesieve_free_iterator(primesieve_iterator *it);
 void primesieve_jump_to(primesieve_iterator *it, uint64_t start, uint64_t stop_hint);
 uint64_t primesieve_next_prime(primesieve_iterator *it);
 void primesieve_generate_next_primes(primesieve_iterator *it);   /* primes[0..size), i = 0 */
+uint64_t primesieve_prev_prime(primesieve_iterator *it);         /* 0 below 2 */
 void *primesieve_generate_primes(uint64_t start, uint64_t stop, size_t *size, int type);
 void primesieve_free(void *primes);
 uint64_t primesieve_count_primes(uint64_t start, uint64_t stop);

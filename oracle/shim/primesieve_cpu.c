@@ -13,13 +13,15 @@ size_t or_primes_range(uint64_t lo, uint64_t hi, uint64_t *out, size_t cap, int 
 
 void primesieve_init(primesieve_iterator *it) { memset(it, 0, sizeof *it); }
 
-void primesieve_free_iterator(primesieve_iterator *it) { free(it->primes); memset(it, 0, sizeof *it); }
+void primesieve_free_iterator(primesieve_iterator *it) { free(it->primes); free(it->pbuf); memset(it, 0, sizeof *it); }
 
 void primesieve_jump_to(primesieve_iterator *it, uint64_t start, uint64_t stop_hint)
 {
     it->i = it->size = 0;
     it->next_lo = start;
     it->stop_hint = stop_hint;
+    it->pi = 0;
+    it->prev_hi = start + 1;          /* prev_prime starts with the last prime <= start */
 }
 
 static void refill(primesieve_iterator *it)
@@ -34,6 +36,19 @@ static void refill(primesieve_iterator *it)
         it->size = or_primes_range(lo, hi, it->primes, cap, 1);
         it->next_lo = hi;
     }
+}
+
+uint64_t primesieve_prev_prime(primesieve_iterator *it)
+{
+    while (it->pi == 0) {
+        if (it->prev_hi <= 2) return 0;
+        const uint64_t hi = it->prev_hi, lo = hi > CHUNK ? hi - CHUNK : 0;
+        const size_t cap = (size_t)((hi - lo) / 2 + 8);
+        if (it->pcap < cap) { it->pbuf = realloc(it->pbuf, cap * 8); it->pcap = cap; }
+        it->pi = or_primes_range(lo, hi, it->pbuf, cap, 1);
+        it->prev_hi = lo;
+    }
+    return it->pbuf[--it->pi];
 }
 
 void primesieve_generate_next_primes(primesieve_iterator *it)

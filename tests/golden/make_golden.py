@@ -7,7 +7,8 @@ ref_vectors.json   known answers held by the reference's own sources, extracted 
                    A350826/a350826.c, pi tables and windows of A158939/cuda/a158939_cuda.cu,
                    pi(1e9) of A001220/wieferich.c, twin counts of A007508/README.md, the
                    base-2 Wieferich primes of A001220/wieferich.c, the known terms of
-                   A158939 (A158939/a158939.c:7-10) and A252768 (A252768/a252768.c:8-9))
+                   A158939 (A158939/a158939.c:7-10) and A252768 (A252768/a252768.c:8-9), and the
+                   A016045 table of gapchain/README.md (first heads of chains of gaps 2, 4, 6, ...))
 verify_py.json     windows computed by the reference's independent Python verifiers
                    (A001220/verify_wieferich.py, A350826/verify_a350826.py) run here
 configs.json       the full-size workloads computed by the oracle (tests/ checks the oracle
@@ -91,6 +92,10 @@ def ref_vectors():
     g = src("A252768/a252768.c")
     m = re.search(r"Terms: a\(1\.\.7\) = ([\d, ]+) \(OEIS, 2014\);\n \*\s+a\(8\) = (\d+) and a\(9\) = (\d+)", g)
     out["A252768"] = [int(x) for x in m.group(1).split(",")] + [int(m.group(2)), int(m.group(3))]
+    g = src("gapchain/README.md")
+    sec = g.split("## Relation to OEIS A016045", 1)[1].split("\n## ", 1)[0]
+    rows = re.findall(r"^\|\s*(\d+)\s*\|\s*(\d+)\s*\|\s*\**([\d,]+)\**", sec, re.M)
+    out["A016045"] = [int(v.replace(",", "")) for n, l, v in rows]
     return out
 
 
