@@ -156,6 +156,14 @@ int mp_gap_stats_range(mp_handle *h, uint64_t lo, uint64_t hi, mp_gap_stats *out
 int mp_gap_chains(mp_handle *h, uint64_t lo, uint64_t hi, uint32_t min_len, uint64_t *heads, uint32_t *lens,
                   size_t cap, size_t *count);
 
+/* the same list (4 <= k < MP_CHAIN_MAX, hi <= 2^63) by the constellation sieve, which does not
+ * enumerate primes: residue classes of a wheel, rotated bit patterns of the primes up to 199
+ * over every member, base-2 strong tests of the survivors' members, and exact verification
+ * (BPSW on members and on the odd numbers between them).  The method of gapchain/gapsieve.c
+ * (gapchain/README_SIEVE.md); heads below 2^24 are found by enumeration. */
+int mp_chain_sieve(mp_handle *h, uint64_t lo, uint64_t hi, uint32_t k, uint64_t *heads, uint32_t *lens,
+                   size_t cap, size_t *count);
+
 /* ---- BPSW ----
  * verdict bit i (bit i & 7 of byte i >> 3) = 1 iff n[i] is prime.  For n < 2^64 this is
  * BPSW (base-2 strong test + strong Lucas test with Selfridge's parameters) after trial

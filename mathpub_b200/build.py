@@ -15,8 +15,8 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmathpub.so")
 WORK = os.path.join(HERE, "libmpwork.so")
 SOURCES = ["mp_api.cu", "mp_sieve.cu", "mp_bpsw.cu", "mp_fermat.cu", "mp_tune.cu", "mp_serve.cu", "mp_probe.cu",
-           "mp_primesieve.cu", "mp_gap.cu"]
-HEADERS = ["mp_common.cuh"]
+           "mp_primesieve.cu", "mp_gap.cu", "mp_chain.cu"]
+HEADERS = ["mp_common.cuh", "mp_mont64.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

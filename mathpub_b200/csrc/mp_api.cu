@@ -96,6 +96,7 @@ int mp_free(mp_handle *h)
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
     mp_graphs_free(h);
+    mp_chain_free(h);
     DevBuf *bufs[] = {&h->tilesum, &h->blockacc, &h->rec, &h->reccnt, &h->queue, &h->errflag, &h->scratch_bitmap,
                       &h->bpsw_n, &h->bpsw_bits, &h->ferm_p, &h->ferm_q, &h->ferm_part, &h->stats_out, &h->small_out,
                       &h->boot.q, &h->boot.magic, &h->table.q, &h->table.magic, &h->scat_bounds, &h->tstate, &h->gap_acc};

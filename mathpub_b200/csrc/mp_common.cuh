@@ -172,6 +172,7 @@ struct Autotune {
 };
 
 struct GraphCache;
+struct ChainDev;                     // the constellation sieve's plan and buffers (mp_chain.cu)
 
 // per-kernel timing for measurement: when enabled, each launch of a timed kernel category is
 // bracketed by CUDA events on its own stream; mp_profile_read sums them
@@ -210,6 +211,7 @@ struct mp_handle {
 
     Autotune tune;
     GraphCache *graphs = nullptr;
+    ChainDev *chain = nullptr;
 
     u64 buf_gen = 0;                 // bumped by every scratch reallocation
     bool prof_on = false;
@@ -295,3 +297,4 @@ int mp_fermat_run(mp_handle *h, const u64 *d_p, u64 count, u64 *d_q, cudaStream_
 int mp_fermat_reduce(mp_handle *h, const u64 *d_p, const u64 *d_q, u64 count,
                      mp_wief_stats *d_stats, cudaStream_t st);
 void mp_graphs_free(mp_handle *h);                                   // mp_api.cu
+void mp_chain_free(mp_handle *h);                                    // mp_chain.cu
