@@ -156,13 +156,23 @@ int mp_gap_stats_range(mp_handle *h, uint64_t lo, uint64_t hi, mp_gap_stats *out
 int mp_gap_chains(mp_handle *h, uint64_t lo, uint64_t hi, uint32_t min_len, uint64_t *heads, uint32_t *lens,
                   size_t cap, size_t *count);
 
-/* the same list (4 <= k < MP_CHAIN_MAX, hi <= 2^63) by the constellation sieve, which does not
- * enumerate primes: residue classes of a wheel, rotated bit patterns of the primes up to 199
- * over every member, base-2 strong tests of the survivors' members, and exact verification
- * (BPSW on members and on the odd numbers between them).  The method of gapchain/gapsieve.c
- * (gapchain/README_SIEVE.md); heads below 2^24 are found by enumeration. */
-int mp_chain_sieve(mp_handle *h, uint64_t lo, uint64_t hi, uint32_t k, uint64_t *heads, uint32_t *lens,
-                   size_t cap, size_t *count);
+/* chains by the constellation sieve, which enumerates no primes: residue classes of a wheel,
+ * rotated bit patterns of the primes up to 199 over every member, base-2 strong tests of the
+ * survivors' members, then exact verification on the GPU (BPSW on the members and on the odd
+ * numbers between them).  The method of gapchain/gapsieve.c (gapchain/README_SIEVE.md).
+ *   shape MP_CHAIN_INC: gaps 2, 4, 6, ... (A016045); the same heads and lengths as
+ *                       mp_gap_chains(lo, hi, k) (2 <= k < MP_CHAIN_MAX; k < 4 is enumerated)
+ *   shape MP_CHAIN_DEC: gaps ..., 6, 4, 2 (A263049; 4 <= k < MP_CHAIN_MAX).  A chain is found
+ *                       by its k-prime pattern p, p + 2(k-1), ..., which ends it, and is
+ *                       reported from its first prime with its full length, as the reference's
+ *                       gapchain_ps.c:365-395 and gapsieve.c:888-916 do; p (the key) lies in
+ *                       [lo, hi), the first prime may lie below lo
+ * heads[] ascending, lens[] capped at MP_CHAIN_MAX - 1; *count = the number of chains. */
+#define MP_CHAIN_INC 0u
+#define MP_CHAIN_DEC 1u
+#define MP_CHAIN_SIEVE_HI_MAX (0xffffffffffffffffull - 4095ull)   /* 2^64 - 2^12 */
+int mp_chain_sieve(mp_handle *h, uint64_t lo, uint64_t hi, uint32_t k, uint32_t shape, uint64_t *heads,
+                   uint32_t *lens, size_t cap, size_t *count);
 
 /* ---- BPSW ----
  * verdict bit i (bit i & 7 of byte i >> 3) = 1 iff n[i] is prime.  For n < 2^64 this is

@@ -117,7 +117,7 @@ def lib():
             "mp_wieferich_stats_noalloc": ([vp, vp, u64, vp, vp], C.c_int),
             "mp_gap_stats_range": ([vp, u64, u64, vp], C.c_int),
             "mp_gap_chains": ([vp, u64, u64, u32, vp, vp, C.c_size_t, C.POINTER(C.c_size_t)], C.c_int),
-            "mp_chain_sieve": ([vp, u64, u64, u32, vp, vp, C.c_size_t, C.POINTER(C.c_size_t)], C.c_int),
+            "mp_chain_sieve": ([vp, u64, u64, u32, u32, vp, vp, C.c_size_t, C.POINTER(C.c_size_t)], C.c_int),
             "mp_autotune": ([vp, u64, C.c_char_p, C.c_size_t], C.c_int),
             "mp_profile_enable": ([vp, C.c_int], C.c_int),
             "mp_profile_read": ([vp, vp, vp, C.c_int], C.c_int),
@@ -274,14 +274,17 @@ class Engine:
         self._check(lib().mp_gap_chains(self._h, lo, hi, min_len, _p(heads), _p(lens), n.value, C.byref(n)))
         return heads[:n.value], lens[:n.value]
 
-    def chain_sieve(self, lo, hi, k):
-        """The same heads and lengths as gap_chains(lo, hi, k), found by the constellation sieve
-        (mp_chain_sieve; 4 <= k < 32)."""
+    def chain_sieve(self, lo, hi, k, dec=False):
+        """Chains of at least k consecutive primes by the constellation sieve (mp_chain_sieve):
+        gaps 2, 4, 6, ... (the same heads and lengths as gap_chains), or with dec=True gaps
+        ..., 6, 4, 2, keyed by the k-prime pattern that ends the chain and reported from the
+        chain's first prime.  Returns (heads, lens) in ascending order of head."""
         n = C.c_size_t()
-        self._check(lib().mp_chain_sieve(self._h, lo, hi, k, None, None, 0, C.byref(n)))
+        shape = 1 if dec else 0
+        self._check(lib().mp_chain_sieve(self._h, lo, hi, k, shape, None, None, 0, C.byref(n)))
         heads = np.zeros(max(1, n.value), dtype=np.uint64)
         lens = np.zeros(max(1, n.value), dtype=np.uint32)
-        self._check(lib().mp_chain_sieve(self._h, lo, hi, k, _p(heads), _p(lens), n.value, C.byref(n)))
+        self._check(lib().mp_chain_sieve(self._h, lo, hi, k, shape, _p(heads), _p(lens), n.value, C.byref(n)))
         return heads[:n.value], lens[:n.value]
 
     def wieferich_range(self, lo, hi):

@@ -31,7 +31,7 @@ def _stale():
         return True
     t = os.path.getmtime(LIB)
     deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS] + [os.path.join(ROOT, "include", h)
-                                                                  for h in ("mathpub_gpu.h", "primesieve.h")]
+                                                                  for h in ("mathpub_gpu.h", "primesieve.h", "gapsieve_cuda.h")]
     return any(os.path.getmtime(d) > t for d in deps)
 
 

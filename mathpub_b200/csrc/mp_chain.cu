@@ -1,80 +1,216 @@
-// mp_chain.cu -- the constellation sieve for chains of consecutive primes with gaps 2, 4, 6,
-// ... (A016045): the heads p whose members p + m(m + 1), m < k, are all prime with nothing
-// prime in between.  It finds what mp_gap_chains finds by enumeration without enumerating
-// primes; the method is the one gapchain/README_SIEVE.md describes for gapchain/gapsieve.c.
+// mp_chain.cu -- the constellation sieve for chains of consecutive primes with gaps 2, 4, 6, ...
+// (A016045) and with gaps ..., 6, 4, 2 (A263049), without enumerating primes.  The method is
+// the one gapchain/README_SIEVE.md describes for gapchain/gapsieve.c:
 //
 //   wheel     the residues of p modulo the primes 2..q_w that leave every member coprime to
-//             them, combined by CRT into the classes s0 of p mod W (W = 2 3 5 ... q_w, grown
-//             while W <= 3e7 and the classes number at most 24,000); p = b + s0 + k W
-//   patterns  for the primes q above the wheel up to 199: member m is divisible by q exactly
-//             when (k + t + s0 W^-1) mod q = -m(m + 1) W^-1 mod q, t = b / W.  The forbidden
-//             residues of each group of primes (periods multiplied up to 2^24) are one bit
-//             pattern; a class reads it from the rotation (t + C) mod P, C = CRT(s0 W^-1), so
-//             2^17 values of k cost a few 64-bit window reads and ANDs per word
-//   screen    the survivors' members in order with the base-2 strong test; a composite
-//             verdict is exact
-//   verify    every member certified by BPSW (exact below 2^64), every odd number between
-//             consecutive members composite, and the chain extended past k
-// Heads below 2^24 (where a member could be a sieving prime) come from mp_gap_chains.
+//             them, combined by CRT into the admissible classes mod W; a segment of 2^17 W
+//             integers from `base` holds, in class j, p = base + s0 + kW, s0 = (res_j - base)
+//             mod W, k < 2^17
+//   patterns  for each sieve prime q above the wheel, member o of p is divisible by q exactly
+//             when k + r = -W^-1 o (mod q), r = W^-1 (base + s0) mod q.  The forbidden
+//             residues of a group of primes (period P = their product) make one bit pattern,
+//             which a class reads from the rotation R = CRT(r) mod P, so 2^17 values of k cost
+//             a few 64-bit window reads and ANDs per word (gapsieve.c:1136-1180)
+//   screen    every member of every survivor by the base-2 strong test (a composite verdict
+//             is a proof): one member at a time over the whole list with compaction between
+//             rounds, then the remaining members per candidate
+//   verify    members prime (exact), the odd numbers between them composite, the chain
+//             extended (forwards for gaps 2, 4, ...; backwards for ..., 4, 2, whose pattern
+//             ends every chain it is part of)
+//
+// Two front ends share the kernels:
+//   cu_*            the C ABI of gapchain/gapsieve_cuda.h (include/gapsieve_cuda.h), so the
+//                   reference's host program gapchain/gapsieve_cuda_host.c runs unmodified on
+//                   these kernels; its host builds the tables and proves the survivors, up to
+//                   its ceiling 3.3e24 (two-word Montgomery arithmetic above 2^64)
+//   mp_chain_sieve  this library's call: the same tables built here, verification on the GPU
+//                   with BPSW, the chains returned in order like mp_gap_chains
 #include "mp_mont64.cuh"
 #include <algorithm>
 #include <numeric>
+#include "../../include/gapsieve_cuda.h"
 
-#define CH_K 131072u                          // k values per class and segment
-#define CH_WORDS (CH_K / 64)
-#define CH_PMAX 199u                          // pattern primes up to this
-#define CH_PERIOD_MAX (1u << 24)
-#define CH_LOW ((u64)1 << 24)                 // heads below this come from the enumeration
-#define CH_MAXG 24
+#define CS_K 131072u                          // values of k per class and segment
+#define CS_WORDS (CS_K / 64)
+#define CS_THREADS 256u
+#define CS_WPT (CS_WORDS / CS_THREADS)       // words per thread
+#define CS_MAXG 64                            // pattern groups
+#define CS_SIEVE_LO 1024u                     // mp_chain_sieve: heads below this are checked one by one
+#define CS_PMAX 199u                          // mp_chain_sieve: pattern primes up to this
+#define CS_PERIOD_MAX (1u << 24)
+#define CS_MAXLEN (MP_CHAIN_MAX - 1)
+#define CS_NCNT (CU_MAXK + 2)                 // counters per shape: raw, after each round, final
 
-struct ChainSieveArgs {
-    u64 b0;                                    // segment 0 starts at b0 (a multiple of W)
-    u64 W;
-    u32 nclass, ngroup, seg0, nseg;           // segments [seg0, seg0 + nseg)
-    u64 lo, hi;                               // heads in [lo, hi)
-    const u32 *s0;                            // [nclass]
-    const u32 *C;                             // [nclass][ngroup]
-    const u64 *pat[CH_MAXG];                  // group patterns
-    u32 period[CH_MAXG];
-    u32 tmod[CH_MAXG];                        // (b0 / W + seg0 * CH_K) mod period
-    u64 *cand;
-    u64 cap;
-    unsigned long long *ncand;
+typedef unsigned __int128 u128t;
+typedef unsigned long long ull;
+
+// ---- two-word Montgomery arithmetic (R = 2^128) for odd n < 2^127 ----
+
+struct w2 { u64 lo, hi; };
+
+__device__ __forceinline__ bool w2_ge(w2 a, w2 b) { return a.hi != b.hi ? a.hi > b.hi : a.lo >= b.lo; }
+__device__ __forceinline__ bool w2_eq(w2 a, w2 b) { return a.hi == b.hi && a.lo == b.lo; }
+__device__ __forceinline__ w2 w2_sub(w2 a, w2 b) { return w2{a.lo - b.lo, a.hi - b.hi - (a.lo < b.lo)}; }
+// a + b mod n for a, b < n < 2^127 (the sum fits in 128 bits)
+__device__ __forceinline__ w2 w2_madd(w2 a, w2 b, w2 n)
+{
+    w2 s;
+    s.lo = a.lo + b.lo;
+    s.hi = a.hi + b.hi + (s.lo < a.lo);
+    return w2_ge(s, n) ? w2_sub(s, n) : s;
+}
+// CIOS product a b 2^-128 mod n for a, b < n; ni = -n^-1 mod 2^64.  After each word of b the
+// running sum is below 2n, so three words hold it and one subtraction finishes.
+__device__ __forceinline__ w2 w2_mmul(w2 a, w2 b, w2 n, u64 ni)
+{
+    u64 t0, t1, t2, m;
+    u128t p;
+    p = (u128t)a.lo * b.lo;                       t0 = (u64)p;
+    p = (u128t)a.hi * b.lo + (u64)(p >> 64);      t1 = (u64)p; t2 = (u64)(p >> 64);
+    m = t0 * ni;
+    p = (u128t)m * n.lo + t0;
+    p = (u128t)m * n.hi + t1 + (u64)(p >> 64);    t0 = (u64)p;
+    p = (u128t)t2 + (u64)(p >> 64);               t1 = (u64)p; t2 = (u64)(p >> 64);
+    p = (u128t)a.lo * b.hi + t0;                  t0 = (u64)p;
+    p = (u128t)a.hi * b.hi + t1 + (u64)(p >> 64); t1 = (u64)p; t2 += (u64)(p >> 64);
+    m = t0 * ni;
+    p = (u128t)m * n.lo + t0;
+    p = (u128t)m * n.hi + t1 + (u64)(p >> 64);    t0 = (u64)p;
+    p = (u128t)t2 + (u64)(p >> 64);               t1 = (u64)p; t2 = (u64)(p >> 64);
+    const w2 r{t0, t1};
+    return (t2 || w2_ge(r, n)) ? w2_sub(r, n) : r;
+}
+
+// the base-2 strong probable-prime test, odd 3 <= n < 2^127
+__device__ bool sprp2_w2(w2 n)
+{
+    const u64 ni = 0 - m_inv(n.lo);
+    // 1 in Montgomery form, 2^128 mod n, by doubling 2^b (b = the top bit of n, so 2^b < n)
+    const int b = n.hi ? 127 - __clzll((long long)n.hi) : 63 - __clzll((long long)n.lo);
+    w2 one = b >= 64 ? w2{0, 1ull << (b - 64)} : w2{1ull << b, 0};
+    for (int i = b; i < 128; i++) one = w2_madd(one, one, n);
+    w2 d = w2_sub(n, w2{1, 0});
+    int s = 0;
+    if (!d.lo) { s = 64; d.lo = d.hi; d.hi = 0; }
+    const int z = __ffsll((long long)d.lo) - 1;
+    if (z) { d.lo = (d.lo >> z) | (d.hi << (64 - z)); d.hi >>= z; }
+    s += z;
+    const w2 mone = w2_sub(n, one);
+    w2 x = w2_madd(one, one, n);              // 2, for the top bit of d
+    const int top = d.hi ? 127 - __clzll((long long)d.hi) : 63 - __clzll((long long)d.lo);
+    for (int i = top - 1; i >= 0; i--) {
+        x = w2_mmul(x, x, n, ni);
+        const u64 bit = i >= 64 ? (d.hi >> (i - 64)) & 1 : (d.lo >> i) & 1;
+        if (bit) x = w2_madd(x, x, n);
+    }
+    if (w2_eq(x, one) || w2_eq(x, mone)) return true;
+    for (int i = 1; i < s; i++) {
+        x = w2_mmul(x, x, n, ni);
+        if (w2_eq(x, mone)) return true;
+        if (w2_eq(x, one)) return false;
+    }
+    return false;
+}
+
+// the base-2 strong test of the member base + off + o (128-bit sum, odd, >= 3)
+__device__ __forceinline__ bool member_sprp2(u64 base_lo, u64 base_hi, u64 off, u32 o)
+{
+    u64 lo = base_lo + off;
+    u64 hi = base_hi + (lo < off);
+    const u64 l2 = lo + o;
+    hi += l2 < lo;
+    lo = l2;
+    if (!hi) return sprp2_dev(lo, m_inv(lo), m_one(lo));
+    return sprp2_w2(w2{lo, hi});
+}
+
+// exact primality for any u64: trial division below 2^20, BPSW above (no pseudoprime below 2^64)
+__device__ bool is_prime_exact(u64 x)
+{
+    if (x < 4) return x >= 2;
+    if (!(x & 1)) return false;
+    if (x < (1u << 20)) {
+        const u32 y = (u32)x;
+        for (u32 d = 3; d * d <= y; d += 2)
+            if (y % d == 0) return false;
+        return true;
+    }
+    return bpsw_odd(x);
+}
+
+// ---- the kernels ----
+
+struct CsTables {                             // shared by both shapes and every unit
+    const u32 *ginfo;                         // per group: P, first sieve prime, primes, word offset
+    const u32 *q, *qinv, *crt;                // per sieve prime: q, W^-1 mod q, CRT coefficient mod P
+    u32 ngroups, nps;
+};
+struct CsShape {
+    const u64 *pat;                           // the groups' patterns back to back
+    const u32 *res;                           // admissible residues mod W
+    const u32 *offs;                          // member offsets
+    u32 A, k;
+};
+struct CsUnit {
+    u64 base_lo, base_hi;                     // segment 0 starts here
+    u64 lim;                                  // the largest candidate offset in range
+    u64 segsize;                              // CS_K W
+    u32 W, bmodW, nseg;
+    u32 j0, nj;                               // classes j0 .. j0 + nj - 1
+    const u32 *bq;                            // [segment][sieve prime]: the segment's base mod q
 };
 
-// one CTA per (class, segment): AND the rotated group patterns over the segment's 2^17 values
-// of k and append the survivors' p
-__global__ void __launch_bounds__(256) chain_sieve_kernel(ChainSieveArgs a)
+// one CTA per (class, segment): AND the rotated patterns over the segment's 2^17 values of k
+// and append the survivors' offsets from the unit's base.  Word w = thread + 256 i is coalesced
+// across the warp; a word that is already 0 loads nothing from the later groups.
+__global__ void __launch_bounds__(CS_THREADS) cs_sieve_kernel(CsTables T, CsShape S, CsUnit U, u64 *list, u64 cap,
+                                                              ull *count)
 {
-    const u32 c = blockIdx.x % a.nclass, s = blockIdx.x / a.nclass;
-    const u64 base = a.b0 + (u64)(a.seg0 + s) * CH_K * a.W + a.s0[c];
-    const u32 lane = threadIdx.x & 31;
-    for (u32 w = threadIdx.x; w < CH_WORDS; w += blockDim.x) {
-        u64 acc = ~0ull;
-        for (u32 g = 0; g < a.ngroup; g++) {
-            const u32 P = a.period[g];
-            // rotation of this class and segment, then the word's first bit
-            u64 y = (u64)a.tmod[g] + (u64)s * (CH_K % P) + a.C[(u64)c * a.ngroup + g];
-            y %= P;
-            y += 64ull * w;
-            const u64 *pw = a.pat[g] + (y >> 6);
-            const u32 sh = (u32)(y & 63);
-            const u64 lo64 = __ldg(pw), hi64 = __ldg(pw + 1);
-            acc &= sh ? (lo64 >> sh) | (hi64 << (64 - sh)) : lo64;
+    __shared__ u32 s_word[CS_MAXG];
+    __shared__ u32 s_sh[CS_MAXG];
+    const u32 j = U.j0 + blockIdx.x % U.nj, g = blockIdx.x / U.nj;
+    const u32 r = S.res[j];
+    const u32 s0 = r >= U.bmodW ? r - U.bmodW : r + U.W - U.bmodW;
+    const u32 *bq = U.bq + (size_t)g * T.nps;
+    for (u32 gi = threadIdx.x; gi < T.ngroups; gi += CS_THREADS) {
+        const u32 P = T.ginfo[4 * gi], first = T.ginfo[4 * gi + 1], n = T.ginfo[4 * gi + 2];
+        u64 R = 0;
+        for (u32 i = first; i < first + n; i++) {
+            const u32 q = T.q[i];
+            u32 t = bq[i] + s0 % q;
+            if (t >= q) t -= q;
+            R += (u64)T.qinv[i] * t % q * T.crt[i];
         }
-        // heads in [lo, hi) only (a word's 64 values span 63 W)
-        const u64 p0 = base + 64ull * w * a.W;
-        if (p0 < a.lo || p0 + 63 * a.W >= a.hi) {
-            u64 bits = acc;
-            while (bits) {
-                const u32 b = __ffsll((long long)bits) - 1;
-                bits &= bits - 1;
-                const u64 p = p0 + (u64)b * a.W;
-                if (p < a.lo || p >= a.hi) acc &= ~(1ull << b);
+        R %= P;
+        s_word[gi] = T.ginfo[4 * gi + 3] + (u32)(R >> 6);
+        s_sh[gi] = (u32)(R & 63);
+    }
+    __syncthreads();
+    u64 acc[CS_WPT];
+#pragma unroll
+    for (u32 i = 0; i < CS_WPT; i++) acc[i] = ~0ull;
+    for (u32 gi = 0; gi < T.ngroups; gi++) {
+        const u64 *pw = S.pat + s_word[gi] + threadIdx.x;
+        const u32 sh = s_sh[gi];
+#pragma unroll
+        for (u32 i = 0; i < CS_WPT; i++)
+            if (acc[i]) {
+                const u64 lo64 = __ldg(pw + CS_THREADS * i), hi64 = __ldg(pw + CS_THREADS * i + 1);
+                acc[i] &= (lo64 >> sh) | ((hi64 << 1) << (63 - sh));   // sh = 0 takes nothing from hi64
             }
+    }
+    const u64 off0 = (u64)g * U.segsize + s0;
+    const u32 lane = threadIdx.x & 31;
+#pragma unroll
+    for (u32 i = 0; i < CS_WPT; i++) {
+        u64 m = acc[i];
+        const u64 o0 = off0 + 64ull * (threadIdx.x + CS_THREADS * i) * U.W;
+        if (m && o0 + 63ull * U.W > U.lim) {                           // the unit's end
+            const u64 room = o0 > U.lim ? 0 : (U.lim - o0) / U.W + 1;  // bits 0 .. room - 1 are in range
+            if (room < 64) m &= (1ull << room) - 1;
         }
-        const u32 nb = __popcll(acc);
-        // warp-aggregated append (every thread takes CH_WORDS / blockDim.x words: all lanes here)
+        const u32 nb = __popcll(m);
+        if (!__ballot_sync(0xffffffffu, nb)) continue;                 // warp-uniform
         u32 incl = nb;
 #pragma unroll
         for (int d = 1; d < 32; d <<= 1) {
@@ -82,65 +218,141 @@ __global__ void __launch_bounds__(256) chain_sieve_kernel(ChainSieveArgs a)
             if (lane >= (u32)d) incl += v;
         }
         const u32 tot = __shfl_sync(0xffffffffu, incl, 31);
-        unsigned long long bpos = 0;
-        if (lane == 31 && tot) bpos = atomicAdd(a.ncand, (unsigned long long)tot);
+        ull bpos = 0;
+        if (lane == 31) bpos = atomicAdd(count, (ull)tot);
         bpos = __shfl_sync(0xffffffffu, bpos, 31);
         u64 pos = bpos + incl - nb;
-        while (acc) {
-            const u32 b = __ffsll((long long)acc) - 1;
-            acc &= acc - 1;
-            if (pos < a.cap) a.cand[pos] = p0 + (u64)b * a.W;
+        while (m) {
+            const u32 b = __ffsll((long long)m) - 1;
+            m &= m - 1;
+            if (pos < cap) list[pos] = o0 + (u64)b * U.W;
             pos++;
         }
     }
 }
 
-// the base-2 strong test on every member, in order; survivors go to the passer list
-__global__ void __launch_bounds__(256) chain_screen_kernel(const u64 *__restrict__ cand, u64 n, u32 k, u64 *pass,
-                                                           u64 cap, unsigned long long *npass)
+// warp-aggregated append (every lane of the warp takes part)
+__device__ __forceinline__ void cs_append(bool keep, u64 v, u64 *out, ull *nout)
 {
-    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
-        const u64 p = cand[i];
-        bool ok = true;
-        for (u32 m = 0; m < k && ok; m++) {
-            const u64 x = p + (u64)m * (m + 1);
-            ok = sprp2_dev(x, m_inv(x), m_one(x));
-        }
-        if (ok) {
-            const unsigned long long j = atomicAdd(npass, 1ull);
-            if (j < cap) pass[j] = p;
-        }
+    const u32 lane = threadIdx.x & 31;
+    const u32 bal = __ballot_sync(0xffffffffu, keep);
+    if (!bal) return;
+    ull base = 0;
+    if (lane == 0) base = atomicAdd(nout, (ull)__popc(bal));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (keep) out[base + __popc(bal & ((1u << lane) - 1))] = v;
+}
+
+// member m over the whole list: keep the offsets whose member passes the base-2 test
+__global__ void __launch_bounds__(256) cs_screen_member(const u64 *__restrict__ in, const ull *nin, u64 cap, u64 *out,
+                                                        ull *nout, u64 base_lo, u64 base_hi, const u32 *offs, u32 m)
+{
+    const u64 n = min((u64)*nin, cap);
+    const u32 o = offs[m];
+    for (u64 i0 = (u64)blockIdx.x * blockDim.x; i0 < n; i0 += (u64)gridDim.x * blockDim.x) {
+        const u64 i = i0 + threadIdx.x;
+        const u64 off = i < n ? in[i] : 0;
+        const bool keep = i < n && member_sprp2(base_lo, base_hi, off, o);
+        cs_append(keep, off, out, nout);
     }
 }
 
-// certify, check the interlopers, extend; chains of at least k primes go to the result list
-__global__ void __launch_bounds__(128) chain_verify_kernel(const u64 *__restrict__ pass, u64 n, u32 k, u64 *heads,
-                                                           u32 *lens, u64 cap, unsigned long long *nres)
+// members m0 .. k - 1 per candidate, stopping at the first composite
+__global__ void __launch_bounds__(256) cs_screen_tail(const u64 *__restrict__ in, const ull *nin, u64 cap, u64 *out,
+                                                      ull *nout, u64 base_lo, u64 base_hi, const u32 *offs, u32 m0,
+                                                      u32 k)
 {
+    const u64 n = min((u64)*nin, cap);
+    for (u64 i0 = (u64)blockIdx.x * blockDim.x; i0 < n; i0 += (u64)gridDim.x * blockDim.x) {
+        const u64 i = i0 + threadIdx.x;
+        const u64 off = i < n ? in[i] : 0;
+        bool keep = i < n;
+        for (u32 m = m0; m < k && keep; m++) keep = member_sprp2(base_lo, base_hi, off, offs[m]);
+        cs_append(keep, off, out, nout);
+    }
+}
+
+// mp_chain_sieve's exact check of the screen's survivors p = base + off (all below 2^64):
+// shape 0 (gaps 2, 4, ...): members p + m(m + 1) prime and the odd numbers between them
+// composite, extended forwards; shape 1 (..., 4, 2): the k-member pattern p + m(2k - 1 - m)
+// exact, then extended backwards while the gap before the first prime is 2 len.  Chains of
+// CS_MAXLEN primes are not extended further.
+__global__ void __launch_bounds__(128) cs_verify_kernel(const u64 *__restrict__ in, const ull *nin, u64 cap, u64 base,
+                                                        u32 k, u32 shape, u64 *heads, u32 *lens, ull *nres)
+{
+    const u64 n = min((u64)*nin, cap);
     for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
-        const u64 p = pass[i];
+        const u64 p = base + in[i];
+        u64 head = p;
         u32 len = 0;
-        // member m is p + m(m + 1); between members m and m + 1 lie the odd numbers
-        // p + m(m + 1) + 2, ..., p + m(m + 1) + 2m
-        for (u32 m = 0; m < MP_CHAIN_MAX - 1; m++) {
-            const u64 x = p + (u64)m * (m + 1);
-            if (!bpsw_odd(x)) break;
-            if (m) {
+        if (shape == 0) {
+            for (u32 m = 0; m < CS_MAXLEN; m++) {
+                const u64 x = p + (u64)m * (m + 1);
+                if (!is_prime_exact(x)) break;
                 bool clear = true;
-                const u64 prev = p + (u64)(m - 1) * m;
-                for (u64 y = prev + 2; y < x && clear; y += 2) clear = !bpsw_odd(y);
+                for (u64 y = x - 2 * (u64)m + 2; m && y < x && clear; y += 2) clear = !is_prime_exact(y);
                 if (!clear) break;
+                len = m + 1;
             }
-            len = m + 1;
+            if (len < k) len = 0;
+        } else {
+            bool ok = true;
+            for (u32 m = 0; m < k && ok; m++) {
+                const u64 x = p + (u64)m * (2 * k - 1 - m);
+                ok = is_prime_exact(x);
+                for (u64 y = x + 2; ok && m + 1 < k && y < x + 2 * (u64)(k - 1 - m); y += 2) ok = !is_prime_exact(y);
+            }
+            if (ok) {
+                len = k;
+                while (len < CS_MAXLEN) {
+                    const u64 gap = 2 * (u64)len;
+                    if (head < gap + 3) break;
+                    const u64 prev = head - gap;
+                    bool step = is_prime_exact(prev);
+                    for (u64 y = prev + 2; step && y < head; y += 2) step = !is_prime_exact(y);
+                    if (!step) break;
+                    head = prev;
+                    len++;
+                }
+            }
         }
-        if (len >= k) {
-            const unsigned long long j = atomicAdd(nres, 1ull);
-            if (j < cap) { heads[j] = p; lens[j] = len; }
+        if (len) {
+            const ull j = atomicAdd(nres, 1ull);
+            if (j < cap) { heads[j] = head; lens[j] = len; }
         }
     }
 }
 
-// ---- host: wheel, patterns, rounds ----
+// all the kernels of one unit of one shape, queued on st.  The survivors end in lists[*fin];
+// counters: cnt[0] the sieve's, cnt[r + 1] after screening round r, cnt[*fcnt] the final one.
+struct CsLists {
+    u64 *list[2];
+    u64 cap;
+    ull *cnt;                                  // CS_NCNT counters
+};
+static void cs_queue_unit(const CsTables &T, const CsShape &S, const CsUnit &U, const CsLists &L, u32 split,
+                          int sm_count, cudaStream_t st, int *fin, u32 *fcnt)
+{
+    const u32 rounds = std::min(split, S.k);
+    cudaMemsetAsync(L.cnt, 0, (size_t)(rounds + 2) * sizeof(ull), st);
+    cs_sieve_kernel<<<U.nj * U.nseg, CS_THREADS, 0, st>>>(T, S, U, L.list[0], L.cap, L.cnt);
+    const unsigned grid = (unsigned)sm_count * 8;
+    int cur = 0;
+    for (u32 r = 0; r < rounds; r++, cur ^= 1)
+        cs_screen_member<<<grid, 256, 0, st>>>(L.list[cur], L.cnt + r, L.cap, L.list[cur ^ 1], L.cnt + r + 1,
+                                               U.base_lo, U.base_hi, S.offs, r);
+    if (rounds < S.k) {
+        cs_screen_tail<<<grid, 256, 0, st>>>(L.list[cur], L.cnt + rounds, L.cap, L.list[cur ^ 1],
+                                             L.cnt + rounds + 1, U.base_lo, U.base_hi, S.offs, rounds, S.k);
+        cur ^= 1;
+        *fcnt = rounds + 1;
+    } else {
+        *fcnt = rounds;
+    }
+    *fin = cur;
+}
+
+// ---- host tables (the reference host builds the same ones for the cu_* path) ----
 
 namespace {
 
@@ -163,117 +375,135 @@ bool is_small_prime(u32 q)
     return true;
 }
 
-struct ChainPlan {
-    u32 k = 0;
+struct CsPlan {
+    u32 k = 0, shape = 0;
     u64 W = 1;
-    std::vector<u32> s0;                        // classes of p mod W
-    std::vector<std::vector<u32>> gq;           // pattern groups
-    std::vector<u32> period;
-    std::vector<u32> C;                         // [class][group]
-    std::vector<std::vector<u64>> pat;          // host copies of the patterns
-    double survive = 1;                         // expected fraction of k surviving the patterns
+    std::vector<u32> res, offs, ginfo, q, qinv, crt;
+    std::vector<u64> pat;
+    double survive = 1;                         // the fraction of k values the patterns keep
 };
 
-// false when some small prime leaves no admissible residue: no chain of length k has a head
-// at or above CH_LOW
-bool make_plan(u32 k, ChainPlan &P)
+// the wheel (grown while W <= 3e7 and the classes number at most 24,000), the pattern groups
+// of the primes above it up to CS_PMAX (periods up to 2^24) and their patterns.  False when
+// some prime leaves no admissible residue: then no chain of this shape and length has a head
+// at or above CS_SIEVE_LO.
+bool make_plan(u32 k, u32 shape, CsPlan &P)
 {
     P.k = k;
-    std::vector<u64> offs(k);
-    for (u32 m = 0; m < k; m++) offs[m] = (u64)m * (m + 1);
+    P.shape = shape;
+    P.offs.resize(k);
+    for (u32 m = 0; m < k; m++) P.offs[m] = shape == 0 ? m * (m + 1) : m * (2 * k - 1 - m);
     std::vector<u64> cls{0};
     u64 W = 1;
     u32 q = 2;
-    for (; q <= CH_PMAX; q++) {
+    for (; q <= CS_PMAX; q++) {
         if (!is_small_prime(q)) continue;
         std::vector<u32> adm;
         for (u32 r = 0; r < q; r++) {
             bool ok = true;
-            for (u64 o : offs) ok = ok && (r + o) % q != 0;
+            for (u32 o : P.offs) ok = ok && (r + o) % q != 0;
             if (ok) adm.push_back(r);
         }
         if (adm.empty()) return false;
         if (q > 2 && (W * q > 30000000ull || cls.size() * adm.size() > 24000)) break;
-        // CRT: x = c (mod W), x = r (mod q)
-        std::vector<u64> nc;
+        std::vector<u64> nc;                    // CRT: x = c (mod W), x = r (mod q)
         const u64 Wi = inv_mod(W % q, q);
         for (u64 c : cls)
-            for (u32 r : adm) {
-                const u64 t = ((r + q - c % q) % q) * Wi % q;
-                nc.push_back(c + W * t);
-            }
+            for (u32 r : adm) nc.push_back(c + W * (((r + q - c % q) % q) * Wi % q));
         cls.swap(nc);
         W *= q;
     }
     std::sort(cls.begin(), cls.end());
     P.W = W;
-    P.s0.assign(cls.begin(), cls.end());
-    // pattern groups from the first prime above the wheel up to CH_PMAX
-    std::vector<u32> gq;
+    P.res.assign(cls.begin(), cls.end());
+    // groups of the next primes up to CS_PMAX
+    std::vector<std::vector<u32>> groups;
+    std::vector<u32> cur;
     u64 per = 1;
-    for (; q <= CH_PMAX; q++) {
+    for (; q <= CS_PMAX; q++) {
         if (!is_small_prime(q)) continue;
-        if (per * q > CH_PERIOD_MAX) { P.gq.push_back(gq); gq.clear(); per = 1; }
-        gq.push_back(q);
+        if (per * q > CS_PERIOD_MAX) { groups.push_back(cur); cur.clear(); per = 1; }
+        cur.push_back(q);
         per *= q;
     }
-    if (!gq.empty()) P.gq.push_back(gq);
-    const u32 G = (u32)P.gq.size();
-    P.period.resize(G);
-    P.pat.resize(G);
-    for (u32 g = 0; g < G; g++) {
+    if (!cur.empty()) groups.push_back(cur);
+    if (groups.size() > CS_MAXG) return false;
+    for (const auto &G : groups) {
         u64 Pg = 1;
-        for (u32 qq : P.gq[g]) Pg *= qq;
-        P.period[g] = (u32)Pg;
-        // forbidden residues per prime, -m(m + 1) W^-1 mod q: strike their classes over one period
+        for (u32 qq : G) Pg *= qq;
+        const u32 first = (u32)P.q.size();
         std::vector<u8> ok(Pg, 1);
-        for (u32 qq : P.gq[g]) {
-            std::vector<char> bad(qq, 0);
+        for (u32 qq : G) {
             const u64 Wi = inv_mod(W % qq, qq);
+            std::vector<u8> bad(qq, 0);
             u32 nbad = 0;
-            for (u64 o : offs) {
-                const u64 f = (qq - (o % qq)) % qq * Wi % qq;
+            for (u32 o : P.offs) {
+                const u64 f = (qq - o % qq) % qq * Wi % qq;          // k + r = -W^-1 o (mod q)
                 if (bad[f]) continue;
                 bad[f] = 1;
                 nbad++;
                 for (u64 y = f; y < Pg; y += qq) ok[y] = 0;
             }
+            if (nbad == qq) return false;
             P.survive *= 1.0 - (double)nbad / qq;
+            const u64 M = Pg / qq;
+            P.q.push_back(qq);
+            P.qinv.push_back((u32)Wi);
+            P.crt.push_back((u32)(M * inv_mod(M % qq, qq) % Pg));
         }
-        // the period, then the first CH_K + 128 bits again, so that no window read wraps
-        const u64 nbits = Pg + CH_K + 128;
-        std::vector<u64> bits((nbits + 63) / 64 + 1, 0);
+        // the period, then its first CS_K + 128 bits again, so that no window read wraps
+        const u64 nbits = Pg + CS_K + 128, nw = (nbits + 63) / 64;
+        const u64 w0 = P.pat.size();
+        P.ginfo.insert(P.ginfo.end(), {(u32)Pg, first, (u32)G.size(), (u32)w0});
+        P.pat.resize(w0 + nw, 0);
         for (u64 y = 0, yy = 0; y < nbits; y++, yy = yy + 1 == Pg ? 0 : yy + 1)
-            if (ok[yy]) bits[y >> 6] |= 1ull << (y & 63);
-        P.pat[g].swap(bits);
+            if (ok[yy]) P.pat[w0 + (y >> 6)] |= 1ull << (y & 63);
     }
-    // per class and group: C = CRT over the group's primes of s0 W^-1 mod q
-    P.C.resize(P.s0.size() * G);
-    for (size_t c = 0; c < P.s0.size(); c++)
-        for (u32 g = 0; g < G; g++) {
-            u64 x = 0, M = 1;
-            for (u32 qq : P.gq[g]) {
-                const u64 r = (u64)P.s0[c] % qq * inv_mod(W % qq, qq) % qq;
-                const u64 t = ((r + qq - x % qq) % qq) * inv_mod(M % qq, qq) % qq;
-                x += M * t;
-                M *= qq;
-            }
-            P.C[c * G + g] = (u32)x;
-        }
     return true;
+}
+
+// LSD radix sort of (head, len) pairs by head, skipping the digits where all heads agree
+void sort_chains(std::vector<u64> &H, std::vector<u32> &L)
+{
+    const size_t n = H.size();
+    if (n < 2) return;
+    std::vector<u64> h2(n);
+    std::vector<u32> l2(n);
+    for (int sh = 0; sh < 64; sh += 11) {
+        std::vector<size_t> cnt(2048, 0);
+        for (u64 v : H) cnt[(v >> sh) & 2047]++;
+        if (*std::max_element(cnt.begin(), cnt.end()) == n) continue;
+        size_t pos = 0;
+        for (size_t &c : cnt) { const size_t t = c; c = pos; pos += t; }
+        for (size_t i = 0; i < n; i++) {
+            const size_t d = cnt[(H[i] >> sh) & 2047]++;
+            h2[d] = H[i];
+            l2[d] = L[i];
+        }
+        H.swap(h2);
+        L.swap(l2);
+    }
+}
+
+template <class T> cudaError_t upload(DevBuf &b, const std::vector<T> &v)
+{
+    cudaError_t e = b.ensure(std::max<size_t>(v.size(), 1) * sizeof(T));
+    if (e == cudaSuccess && !v.empty()) e = cudaMemcpy(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
+    return e;
 }
 
 }  // namespace
 
+// ---- mp_chain_sieve ----
+
 struct ChainDev {
-    u32 k = 0;
-    ChainPlan plan;
-    std::vector<DevBuf> pat;
-    DevBuf s0, C, cand, pass, res, cnt;
+    u32 k = 0, shape = 0;
+    bool ok = false;                           // false: no chain of this shape and length above CS_SIEVE_LO
+    CsPlan plan;
+    DevBuf ginfo, q, qinv, crt, pat, res, offs, bq, l0, l1, cnt, rh, rl;
     void release()
     {
-        for (DevBuf &b : pat) b.release();
-        for (DevBuf *b : {&s0, &C, &cand, &pass, &res, &cnt}) b->release();
+        for (DevBuf *b : {&ginfo, &q, &qinv, &crt, &pat, &res, &offs, &bq, &l0, &l1, &cnt, &rh, &rl}) b->release();
     }
 };
 
@@ -285,129 +515,356 @@ void mp_chain_free(mp_handle *h)
     h->chain = nullptr;
 }
 
-static int chain_round(mp_handle *h, ChainDev &D, u64 lo, u64 hi, u64 b0, u32 seg0, u32 nseg, std::vector<u64> &heads,
-                       std::vector<u32> &lens, cudaStream_t st)
+// verify a survivor list (offsets from base, count on the device) and append the chains
+static int cs_collect(mp_handle *h, ChainDev &D, const u64 *list, const ull *nin, u64 cap, u64 base, u64 expect,
+                      std::vector<u64> &H, std::vector<u32> &L, cudaStream_t st)
 {
-    const ChainPlan &P = D.plan;
-    const u32 nclass = (u32)P.s0.size(), G = (u32)P.period.size();
-    const double expect = (double)nclass * nseg * CH_K * P.survive;
-    const u64 cap = (u64)(2.0 * expect) + (1u << 20);
-    MP_CUDA(h, D.cand.ensure((size_t)cap * 8));
-    MP_CUDA(h, D.cnt.ensure(64));
-    unsigned long long *cnt = D.cnt.as<unsigned long long>();
-    MP_CUDA(h, cudaMemsetAsync(cnt, 0, 64, st));
-    ChainSieveArgs a;
-    memset(&a, 0, sizeof a);
-    a.b0 = b0; a.W = P.W; a.nclass = nclass; a.ngroup = G; a.seg0 = seg0; a.nseg = nseg; a.lo = lo; a.hi = hi;
-    a.s0 = D.s0.as<u32>(); a.C = D.C.as<u32>();
-    for (u32 g = 0; g < G; g++) {
-        a.pat[g] = D.pat[g].as<u64>();
-        a.period[g] = P.period[g];
-        const u64 t0 = b0 / P.W + (u64)seg0 * CH_K;
-        a.tmod[g] = (u32)(t0 % P.period[g]);
-    }
-    a.cand = D.cand.as<u64>(); a.cap = cap; a.ncand = cnt;
-    chain_sieve_kernel<<<nclass * nseg, 256, 0, st>>>(a);
+    ull *nres = D.cnt.as<ull>() + CS_NCNT;
+    MP_CUDA(h, D.rh.ensure(cap * 8));
+    MP_CUDA(h, D.rl.ensure(cap * 4));
+    MP_CUDA(h, cudaMemsetAsync(nres, 0, sizeof(ull), st));
+    const u64 grid = std::max<u64>(1, std::min<u64>((expect + 127) / 128, (u64)h->sm_count * 16));
+    cs_verify_kernel<<<(unsigned)grid, 128, 0, st>>>(list, nin, cap, base, D.k, D.shape, D.rh.as<u64>(), D.rl.as<u32>(),
+                                                     nres);
     MP_CUDA(h, cudaGetLastError());
-    u64 nc = 0;
-    MP_CUDA(h, cudaMemcpyAsync(&nc, cnt, 8, cudaMemcpyDeviceToHost, st));
+    ull nr = 0;
+    MP_CUDA(h, cudaMemcpyAsync(&nr, nres, sizeof nr, cudaMemcpyDeviceToHost, st));
     MP_CUDA(h, cudaStreamSynchronize(st));
-    if (nc > cap) {                                  // more survivors than room: split the round
-        if (nseg == 1) return mp_set_error(h, MP_EOVERFLOW, "chain sieve: survivors exceed the candidate buffer");
-        MP_TRY(chain_round(h, D, lo, hi, b0, seg0, nseg / 2, heads, lens, st));
-        return chain_round(h, D, lo, hi, b0, seg0 + nseg / 2, nseg - nseg / 2, heads, lens, st);
-    }
-    if (!nc) return MP_OK;
-    const u64 pcap = nc / 16 + 4096;
-    MP_CUDA(h, D.pass.ensure((size_t)pcap * 8));
-    u64 grid = std::min<u64>((nc + 255) / 256, (u64)h->sm_count * 64);
-    chain_screen_kernel<<<(unsigned)grid, 256, 0, st>>>(D.cand.as<u64>(), nc, P.k, D.pass.as<u64>(), pcap, cnt + 1);
-    MP_CUDA(h, cudaGetLastError());
-    u64 np = 0;
-    MP_CUDA(h, cudaMemcpyAsync(&np, cnt + 1, 8, cudaMemcpyDeviceToHost, st));
-    MP_CUDA(h, cudaStreamSynchronize(st));
-    if (np > pcap) return mp_set_error(h, MP_EOVERFLOW, "chain sieve: screen passers exceed their buffer");
-    if (!np) return MP_OK;
-    MP_CUDA(h, D.res.ensure((size_t)np * 12 + 64));
-    u64 *rh = D.res.as<u64>();
-    u32 *rl = (u32 *)(rh + np);
-    grid = std::min<u64>((np + 127) / 128, (u64)h->sm_count * 16);
-    chain_verify_kernel<<<(unsigned)grid, 128, 0, st>>>(D.pass.as<u64>(), np, P.k, rh, rl, np, cnt + 2);
-    MP_CUDA(h, cudaGetLastError());
-    u64 nr = 0;
-    MP_CUDA(h, cudaMemcpyAsync(&nr, cnt + 2, 8, cudaMemcpyDeviceToHost, st));
-    MP_CUDA(h, cudaStreamSynchronize(st));
+    if (nr > cap) return mp_set_error(h, MP_EOVERFLOW, "chain sieve: more chains than survivors");
     if (nr) {
-        const size_t o = heads.size();
-        heads.resize(o + nr);
-        lens.resize(o + nr);
-        MP_CUDA(h, cudaMemcpyAsync(heads.data() + o, rh, nr * 8, cudaMemcpyDeviceToHost, st));
-        MP_CUDA(h, cudaMemcpyAsync(lens.data() + o, rl, nr * 4, cudaMemcpyDeviceToHost, st));
+        const size_t o = H.size();
+        H.resize(o + nr);
+        L.resize(o + nr);
+        MP_CUDA(h, cudaMemcpyAsync(H.data() + o, D.rh.p, nr * 8, cudaMemcpyDeviceToHost, st));
+        MP_CUDA(h, cudaMemcpyAsync(L.data() + o, D.rl.p, nr * 4, cudaMemcpyDeviceToHost, st));
         MP_CUDA(h, cudaStreamSynchronize(st));
     }
     return MP_OK;
 }
 
-extern "C" int mp_chain_sieve(mp_handle *h, uint64_t lo, uint64_t hi, uint32_t k, uint64_t *heads, uint32_t *lens,
-                              size_t cap, size_t *count)
+extern "C" int mp_chain_sieve(mp_handle *h, uint64_t lo, uint64_t hi, uint32_t k, uint32_t shape, uint64_t *heads,
+                              uint32_t *lens, size_t cap, size_t *count)
 {
     if (!h || !count || (cap && (!heads || !lens))) return MP_EINVAL;
     *count = 0;
-    if (k < 4 || k >= MP_CHAIN_MAX) return mp_set_error(h, MP_EINVAL, "k must be in 4..%d", MP_CHAIN_MAX - 1);
-    if (hi > (1ull << 63)) return mp_set_error(h, MP_ERANGE, "hi must be <= 2^63");
+    if (shape > 1) return mp_set_error(h, MP_EINVAL, "shape must be MP_CHAIN_INC or MP_CHAIN_DEC");
+    if (k < (shape ? 4u : 2u) || k > CS_MAXLEN)
+        return mp_set_error(h, MP_EINVAL, "k must be in %u..%d", shape ? 4u : 2u, CS_MAXLEN);
+    if (hi > MP_CHAIN_SIEVE_HI_MAX) return mp_set_error(h, MP_ERANGE, "hi must be <= 2^64 - 2^12");
     if (hi <= lo) return MP_OK;
+    if (shape == 0 && k < 4) return mp_gap_chains(h, lo, hi, k, heads, lens, cap, count);   // dense: enumerate
     std::lock_guard<std::recursive_mutex> lk(h->mu);
     MP_CUDA(h, cudaSetDevice(h->device));
     cudaStream_t st = h->stream;
+    if (!h->chain || h->chain->k != k || h->chain->shape != shape) {
+        mp_chain_free(h);
+        h->chain = new ChainDev();
+        ChainDev &D = *h->chain;
+        D.k = k;
+        D.shape = shape;
+        D.ok = make_plan(k, shape, D.plan);
+        const CsPlan &P = D.plan;
+        if (D.ok) {
+            MP_CUDA(h, upload(D.ginfo, P.ginfo));
+            MP_CUDA(h, upload(D.q, P.q));
+            MP_CUDA(h, upload(D.qinv, P.qinv));
+            MP_CUDA(h, upload(D.crt, P.crt));
+            MP_CUDA(h, upload(D.pat, P.pat));
+            MP_CUDA(h, upload(D.res, P.res));
+        }
+        MP_CUDA(h, upload(D.offs, P.offs));
+        MP_CUDA(h, D.cnt.ensure((CS_NCNT + 1) * sizeof(ull)));
+    }
+    ChainDev &D = *h->chain;
+    const CsPlan &P = D.plan;
     std::vector<u64> H;
     std::vector<u32> L;
-    // heads below CH_LOW by enumeration
-    if (lo < CH_LOW) {
-        const u64 e = std::min<u64>(hi, CH_LOW);
-        size_t n = 0;
-        MP_TRY(mp_gap_chains(h, lo, e, k, nullptr, nullptr, 0, &n));
-        H.resize(n);
-        L.resize(n);
-        if (n) MP_TRY(mp_gap_chains(h, lo, e, k, H.data(), L.data(), n, &n));
+    // heads below CS_SIEVE_LO (where a member may be a sieve prime): every odd p, exactly
+    if (lo < CS_SIEVE_LO) {
+        std::vector<u64> strip;
+        for (u64 p = std::max<u64>(lo, 3) | 1; p < std::min<u64>(hi, CS_SIEVE_LO); p += 2) strip.push_back(p);
+        if (!strip.empty()) {
+            MP_CUDA(h, upload(D.l0, strip));
+            const ull n = strip.size();
+            MP_CUDA(h, cudaMemcpy(D.cnt.p, &n, sizeof n, cudaMemcpyHostToDevice));
+            MP_TRY(cs_collect(h, D, D.l0.as<u64>(), D.cnt.as<ull>(), n, 0, n, H, L, st));
+        }
     }
-    const u64 slo = std::max<u64>(lo, CH_LOW);
-    if (slo < hi) {
-        if (!h->chain || h->chain->k != k) {
-            mp_chain_free(h);
-            h->chain = new ChainDev();
-            ChainDev &D = *h->chain;
-            D.k = k;
-            if (make_plan(k, D.plan)) {
-                const ChainPlan &P = D.plan;
-                D.pat.resize(P.pat.size());
-                for (size_t g = 0; g < P.pat.size(); g++) {
-                    MP_CUDA(h, D.pat[g].ensure(P.pat[g].size() * 8));
-                    MP_CUDA(h, cudaMemcpy(D.pat[g].p, P.pat[g].data(), P.pat[g].size() * 8, cudaMemcpyHostToDevice));
+    const u64 slo = std::max<u64>(lo, CS_SIEVE_LO);
+    if (D.ok && slo < hi) {
+        const u64 W = P.W, segsize = (u64)CS_K * W;
+        const u32 A = (u32)P.res.size(), nps = (u32)P.q.size();
+        const u64 nseg_all = (hi - slo + segsize - 1) / segsize;
+        // units: runs of segments (or, for short chains, runs of classes of one segment) sized
+        // for about 2^24 expected sieve survivors
+        const double per_class = (double)CS_K * P.survive, target = 16777216.0;
+        u32 useg = 1, ucls = A;
+        if (per_class * A <= target) useg = (u32)std::min<double>(256.0, std::floor(target / (per_class * A)));
+        else ucls = (u32)std::max<double>(1.0, std::floor(target / per_class));
+        u64 ucap = (u64)(1.25 * per_class * ucls * useg) + 65536;
+        const CsTables T{D.ginfo.as<u32>(), D.q.as<u32>(), D.qinv.as<u32>(), D.crt.as<u32>(),
+                         (u32)(P.ginfo.size() / 4), nps};
+        const CsShape S{D.pat.as<u64>(), D.res.as<u32>(), D.offs.as<u32>(), A, k};
+        std::vector<u32> bq((size_t)useg * nps);
+        MP_CUDA(h, D.bq.ensure(bq.size() * 4));
+        for (u64 s = 0; s < nseg_all; s += useg) {
+            const u32 ns = (u32)std::min<u64>(useg, nseg_all - s);
+            const u64 base = slo + s * segsize;
+            for (u32 g = 0; g < ns; g++)
+                for (u32 i = 0; i < nps; i++) bq[(size_t)g * nps + i] = (u32)((base + g * segsize) % P.q[i]);
+            MP_CUDA(h, cudaMemcpyAsync(D.bq.p, bq.data(), (size_t)ns * nps * 4, cudaMemcpyHostToDevice, st));
+            for (u32 j0 = 0; j0 < A; j0 += ucls) {
+                const CsUnit U{base, 0, hi - 1 - base, segsize, (u32)W, (u32)(base % W), ns, j0,
+                               std::min(ucls, A - j0), D.bq.as<u32>()};
+                for (;;) {
+                    MP_CUDA(h, D.l0.ensure(ucap * 8));
+                    MP_CUDA(h, D.l1.ensure(ucap * 8));
+                    const CsLists Ls{{D.l0.as<u64>(), D.l1.as<u64>()}, ucap, D.cnt.as<ull>()};
+                    int fin = 0;
+                    u32 fcnt = 0;
+                    cs_queue_unit(T, S, U, Ls, 3, h->sm_count, st, &fin, &fcnt);
+                    MP_CUDA(h, cudaGetLastError());
+                    ull raw = 0;
+                    MP_CUDA(h, cudaMemcpyAsync(&raw, D.cnt.p, sizeof raw, cudaMemcpyDeviceToHost, st));
+                    MP_CUDA(h, cudaStreamSynchronize(st));
+                    if (raw > ucap) { ucap = raw + raw / 4 + 65536; continue; }   // lists overflowed: again
+                    MP_TRY(cs_collect(h, D, Ls.list[fin], D.cnt.as<ull>() + fcnt, ucap, base, raw / 8 + 1, H, L, st));
+                    break;
                 }
-                MP_CUDA(h, D.s0.ensure(P.s0.size() * 4));
-                MP_CUDA(h, cudaMemcpy(D.s0.p, P.s0.data(), P.s0.size() * 4, cudaMemcpyHostToDevice));
-                MP_CUDA(h, D.C.ensure(P.C.size() * 4));
-                MP_CUDA(h, cudaMemcpy(D.C.p, P.C.data(), P.C.size() * 4, cudaMemcpyHostToDevice));
-            } else D.plan.s0.clear();             // no chain of length k above CH_LOW
-        }
-        ChainDev &D = *h->chain;
-        if (!D.plan.s0.empty()) {
-            if (D.plan.period.size() > CH_MAXG) return mp_set_error(h, MP_EINVAL, "too many pattern groups");
-            const u64 W = D.plan.W, span = (u64)CH_K * W;
-            const u64 b0 = slo / W * W;
-            const u64 nseg = (hi - b0 + span - 1) / span;
-            // rounds of segments sized for about 2^24 expected survivors
-            const double per = (double)D.plan.s0.size() * CH_K * D.plan.survive;
-            const u32 step = (u32)std::max<double>(1.0, std::min<double>(4096.0, 16777216.0 / per));
-            for (u64 s = 0; s < nseg; s += step)
-                MP_TRY(chain_round(h, D, slo, hi, b0, (u32)s, (u32)std::min<u64>(step, nseg - s), H, L, st));
+            }
         }
     }
-    std::vector<size_t> ord(H.size());
-    std::iota(ord.begin(), ord.end(), 0);
-    std::sort(ord.begin(), ord.end(), [&](size_t x, size_t y) { return H[x] < H[y]; });
+    sort_chains(H, L);
     const size_t m = std::min(cap, H.size());
-    for (size_t i = 0; i < m; i++) { heads[i] = H[ord[i]]; lens[i] = L[ord[i]]; }
+    std::copy(H.begin(), H.begin() + m, heads);
+    std::copy(L.begin(), L.begin() + m, lens);
     *count = H.size();
     return MP_OK;
+}
+
+// ---- the cu_* interface of gapchain/gapsieve_cuda.h ----
+
+namespace {
+
+struct CuSlot {
+    bool set = false, did[2] = {false, false};
+    u32 unit = 0, cap = 0;
+    DevBuf bq, list[2][2], cnt;
+    u32 *h_bq = nullptr;                       // pinned staging, unit x nps
+    ull *h_cnt = nullptr;                      // pinned: raw and final count per shape
+    cudaEvent_t ev = nullptr;
+    int fin[2] = {0, 0};
+    std::vector<u64> host[2];
+};
+
+struct CuState {
+    std::mutex mu;
+    bool init = false;
+    int sm = 0;
+    cudaStream_t st = nullptr, cp = nullptr;   // the units' stream, the list copies' stream
+    DevBuf ginfo, q, qinv, crt;
+    u32 ngroups = 0, nps = 0;
+    struct Shape {
+        DevBuf pat, res, offs;
+        u32 A = 0, k = 0;
+        bool on = false;
+    } sh[2];
+    CuSlot slot[CU_MAXSLOT];
+};
+
+CuState &cu()
+{
+    static CuState s;
+    return s;
+}
+
+int cu_lists(CuSlot &X, u32 cap)
+{
+    CuState &C = cu();
+    for (int d = 0; d < 2; d++)
+        for (int b = 0; b < 2; b++) {
+            X.list[d][b].release();
+            if (C.sh[d].on && X.list[d][b].ensure((size_t)cap * 8) != cudaSuccess) return -1;
+        }
+    X.cap = cap;
+    return 0;
+}
+
+}  // namespace
+
+extern "C" int cu_init(char *name, size_t n)
+{
+    CuState &C = cu();
+    std::lock_guard<std::mutex> lk(C.mu);
+    int nd = 0;
+    if (cudaGetDeviceCount(&nd) != cudaSuccess || nd < 1) return -1;
+    int dev = 0;
+    cudaDeviceProp pr;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaGetDeviceProperties(&pr, dev) != cudaSuccess) return -1;
+    if (name && n) snprintf(name, n, "%s", pr.name);
+    if (!C.init) {
+        if (cudaStreamCreateWithFlags(&C.st, cudaStreamNonBlocking) != cudaSuccess) return -1;
+        if (cudaStreamCreateWithFlags(&C.cp, cudaStreamNonBlocking) != cudaSuccess) return -1;
+        C.sm = pr.multiProcessorCount;
+        C.init = true;
+    }
+    return 0;
+}
+
+extern "C" int cu_tables(uint32_t ngroups, const uint32_t *ginfo, uint32_t nps, const uint32_t *q,
+                         const uint32_t *qinv, const uint32_t *crt)
+{
+    CuState &C = cu();
+    std::lock_guard<std::mutex> lk(C.mu);
+    if (!C.init || !ngroups || ngroups > CS_MAXG || !nps || !ginfo || !q || !qinv || !crt) return -1;
+    const std::vector<u32> gi(ginfo, ginfo + 4 * (size_t)ngroups), qq(q, q + nps), qi(qinv, qinv + nps),
+        cr(crt, crt + nps);
+    if (upload(C.ginfo, gi) || upload(C.q, qq) || upload(C.qinv, qi) || upload(C.crt, cr)) return -1;
+    C.ngroups = ngroups;
+    C.nps = nps;
+    return 0;
+}
+
+extern "C" int cu_shape(int d, const uint32_t *pat, size_t npat, const uint32_t *res, uint32_t A,
+                        const uint32_t *offs, uint32_t k)
+{
+    CuState &C = cu();
+    std::lock_guard<std::mutex> lk(C.mu);
+    if (!C.init || d < 0 || d > 1 || !pat || !npat || (npat & 1) || !res || !A || !offs || !k || k > CU_MAXK) return -1;
+    auto &S = C.sh[d];
+    const std::vector<u32> pv(pat, pat + npat), rv(res, res + A), ov(offs, offs + k);
+    if (upload(S.pat, pv) || upload(S.res, rv) || upload(S.offs, ov)) return -1;
+    S.A = A;
+    S.k = k;
+    S.on = true;
+    return 0;
+}
+
+extern "C" int cu_slot(int slot, uint32_t unit, uint32_t cap)
+{
+    CuState &C = cu();
+    std::lock_guard<std::mutex> lk(C.mu);
+    if (!C.init || slot < 0 || slot >= CU_MAXSLOT || !unit || !cap || !C.nps) return -1;
+    CuSlot &X = C.slot[slot];
+    if (X.bq.ensure((size_t)unit * C.nps * 4) != cudaSuccess) return -1;
+    if (X.cnt.ensure(2 * CS_NCNT * sizeof(ull)) != cudaSuccess) return -1;
+    if (X.h_bq) { cudaFreeHost(X.h_bq); X.h_bq = nullptr; }
+    if (!X.h_cnt && cudaMallocHost(&X.h_cnt, 4 * sizeof(ull)) != cudaSuccess) { X.h_cnt = nullptr; return -1; }
+    if (cudaMallocHost(&X.h_bq, (size_t)unit * C.nps * 4) != cudaSuccess) { X.h_bq = nullptr; return -1; }
+    if (!X.ev && cudaEventCreateWithFlags(&X.ev, cudaEventDisableTiming) != cudaSuccess) return -1;
+    X.unit = unit;
+    if (cu_lists(X, cap)) return -1;
+    X.set = true;
+    return 0;
+}
+
+extern "C" int cu_grow(int slot, uint32_t cap)
+{
+    CuState &C = cu();
+    std::lock_guard<std::mutex> lk(C.mu);
+    if (slot < 0 || slot >= CU_MAXSLOT || !C.slot[slot].set || !cap) return -1;
+    return cu_lists(C.slot[slot], cap);
+}
+
+extern "C" int cu_submit(int slot, const uint32_t *bq, uint32_t nseg, uint32_t nps, const struct cu_params *p[2],
+                         int split)
+{
+    CuState &C = cu();
+    std::lock_guard<std::mutex> lk(C.mu);
+    if (slot < 0 || slot >= CU_MAXSLOT || !bq || !p) return -1;
+    CuSlot &X = C.slot[slot];
+    if (!X.set || !nseg || nseg > X.unit || nps != C.nps) return -1;
+    for (int d = 0; d < 2; d++) {
+        const cu_params *q = p[d];
+        if (!q) continue;
+        const auto &S = C.sh[d];
+        if (!S.on || q->k != S.k || q->A != S.A || q->nps != C.nps || q->ngroups != C.ngroups || q->nseg != nseg ||
+            q->segsize != (u64)CS_K * q->W || q->bmodW >= q->W || q->cap > X.cap)
+            return -1;
+    }
+    memcpy(X.h_bq, bq, (size_t)nseg * nps * 4);
+    if (cudaMemcpyAsync(X.bq.p, X.h_bq, (size_t)nseg * nps * 4, cudaMemcpyHostToDevice, C.st) != cudaSuccess) return -1;
+    const CsTables T{C.ginfo.as<u32>(), C.q.as<u32>(), C.qinv.as<u32>(), C.crt.as<u32>(), C.ngroups, C.nps};
+    for (int d = 0; d < 2; d++) {
+        X.did[d] = p[d] != nullptr;
+        if (!p[d]) continue;
+        const cu_params &q = *p[d];
+        const auto &S0 = C.sh[d];
+        const CsShape S{S0.pat.as<u64>(), S0.res.as<u32>(), S0.offs.as<u32>(), S0.A, S0.k};
+        const CsUnit U{q.base_lo, q.base_hi, q.lim, q.segsize, q.W, q.bmodW, nseg, 0, S0.A, X.bq.as<u32>()};
+        const CsLists L{{X.list[d][0].as<u64>(), X.list[d][1].as<u64>()}, X.cap, X.cnt.as<ull>() + d * CS_NCNT};
+        u32 fcnt = 0;
+        cs_queue_unit(T, S, U, L, split < 0 ? 0u : (u32)split, C.sm, C.st, &X.fin[d], &fcnt);
+        cudaMemcpyAsync(X.h_cnt + 2 * d, L.cnt, sizeof(ull), cudaMemcpyDeviceToHost, C.st);
+        cudaMemcpyAsync(X.h_cnt + 2 * d + 1, L.cnt + fcnt, sizeof(ull), cudaMemcpyDeviceToHost, C.st);
+    }
+    if (cudaEventRecord(X.ev, C.st) != cudaSuccess) return -1;
+    return cudaPeekAtLastError() == cudaSuccess ? 0 : -1;
+}
+
+extern "C" int cu_wait(int slot, uint32_t stat[2], uint32_t nfin[2])
+{
+    CuState &C = cu();
+    if (slot < 0 || slot >= CU_MAXSLOT || !C.slot[slot].set || !stat || !nfin) return -1;
+    CuSlot &X = C.slot[slot];
+    if (cudaEventSynchronize(X.ev) != cudaSuccess) return -1;
+    std::lock_guard<std::mutex> lk(C.mu);
+    for (int d = 0; d < 2; d++) {
+        if (!X.did[d]) continue;
+        const ull raw = X.h_cnt[2 * d], fin = X.h_cnt[2 * d + 1];
+        stat[d] = (u32)std::min<ull>(raw, 0xffffffffull);
+        nfin[d] = (u32)std::min<ull>(fin, X.cap);
+    }
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+extern "C" const uint64_t *cu_list(int slot, int d, uint32_t n)
+{
+    CuState &C = cu();
+    std::lock_guard<std::mutex> lk(C.mu);
+    if (slot < 0 || slot >= CU_MAXSLOT || d < 0 || d > 1) return nullptr;
+    CuSlot &X = C.slot[slot];
+    if (!X.set || !X.did[d] || n > X.cap) return nullptr;
+    X.host[d].resize(std::max<u32>(n, 1));
+    if (n && (cudaMemcpyAsync(X.host[d].data(), X.list[d][X.fin[d]].p, (size_t)n * 8, cudaMemcpyDeviceToHost, C.cp) !=
+                  cudaSuccess ||
+              cudaStreamSynchronize(C.cp) != cudaSuccess))
+        return nullptr;
+    return X.host[d].data();
+}
+
+__global__ void cu_sprp_kernel(const u64 *__restrict__ n, size_t count, u8 *ok)
+{
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (size_t)gridDim.x * blockDim.x) {
+        const u64 lo = n[2 * i], hi = n[2 * i + 1];
+        bool r;
+        if (!hi && lo < 3) r = lo == 2;
+        else if (!(lo & 1)) r = false;
+        else r = member_sprp2(lo, hi, 0, 0);
+        ok[i] = r;
+    }
+}
+
+extern "C" int cu_sprp_batch(const uint64_t *n, size_t count, uint8_t *ok)
+{
+    if (!count) return 0;
+    if (!n || !ok) return -1;
+    for (size_t i = 0; i < count; i++)
+        if (n[2 * i + 1] >> 63) return -1;     // n >= 2^127
+    CuState &C = cu();
+    if (!C.init && cu_init(nullptr, 0)) return -1;
+    DevBuf dn, dk;
+    if (dn.ensure(count * 16) != cudaSuccess || dk.ensure(count) != cudaSuccess) return -1;
+    int rc = 0;
+    if (cudaMemcpyAsync(dn.p, n, count * 16, cudaMemcpyHostToDevice, C.cp) != cudaSuccess) rc = -1;
+    if (!rc) {
+        const unsigned grid = (unsigned)std::max<size_t>(1, std::min<size_t>((count + 255) / 256, (size_t)C.sm * 8));
+        cu_sprp_kernel<<<grid, 256, 0, C.cp>>>(dn.as<u64>(), count, dk.as<u8>());
+        if (cudaMemcpyAsync(ok, dk.p, count, cudaMemcpyDeviceToHost, C.cp) != cudaSuccess ||
+            cudaStreamSynchronize(C.cp) != cudaSuccess)
+            rc = -1;
+    }
+    dn.release();
+    dk.release();
+    return rc;
 }

@@ -272,3 +272,35 @@ def gap_chains(lo, hi, min_len, nthreads=None):
     cl = chain_lengths(np.diff(p), n_in)
     sel = cl >= min_len
     return p[:n_in][sel].astype(np.uint64), np.minimum(cl[sel], CHAIN_MAX - 1).astype(np.uint32)
+
+
+def dec_chains(lo, hi, k, nthreads=None):
+    """Chains of at least k consecutive primes with gaps ..., 6, 4, 2 (A263049), as
+    gapchain/gapchain_ps.c:365-395 finds them: each exact k-prime pattern p, p + 2(k-1), ...,
+    p + (k-1)k of consecutive primes (gaps 2(k-1), ..., 4, 2) with p in [lo, hi) ends a chain,
+    which is extended backwards while the gap before its first prime is 2 len.
+    Returns (first primes ascending, lengths capped at CHAIN_MAX - 1, keys p)."""
+    back = 2 * CHAIN_MAX * CHAIN_MAX
+    p = primes_range(max(0, lo - back), hi + GAP_LOOK, nthreads).astype(np.int64)
+    g = np.diff(p)
+    i0, n_in = int(np.searchsorted(p, lo)), int(np.searchsorted(p, hi))
+    idx = np.arange(i0, n_in)
+    ok = np.ones(len(idx), dtype=bool)
+    for j in range(k - 1):
+        t = idx + j
+        good = t < len(g)
+        step = np.zeros(len(idx), dtype=bool)
+        step[good] = g[t[good]] == 2 * (k - 1 - j)
+        ok &= step
+    heads, lens, keys = [], [], []
+    for i in idx[ok]:
+        h, n = int(i), k
+        while n < CHAIN_MAX - 1 and h > 0 and g[h - 1] == 2 * n:
+            h -= 1
+            n += 1
+        heads.append(int(p[h]))
+        lens.append(n)
+        keys.append(int(p[i]))
+    o = np.argsort(np.array(heads, dtype=np.uint64), kind="stable")
+    return (np.array(heads, dtype=np.uint64)[o], np.array(lens, dtype=np.uint32)[o],
+            np.array(keys, dtype=np.uint64)[o])

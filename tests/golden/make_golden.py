@@ -8,7 +8,8 @@ ref_vectors.json   known answers held by the reference's own sources, extracted 
                    pi(1e9) of A001220/wieferich.c, twin counts of A007508/README.md, the
                    base-2 Wieferich primes of A001220/wieferich.c, the known terms of
                    A158939 (A158939/a158939.c:7-10) and A252768 (A252768/a252768.c:8-9), and the
-                   A016045 table of gapchain/README.md (first heads of chains of gaps 2, 4, 6, ...))
+                   A016045 table of gapchain/README.md (first heads of chains of gaps 2, 4, 6, ...),
+                   its A263049 table (the first starts of the exact patterns of gaps ..., 6, 4, 2))
 verify_py.json     windows computed by the reference's independent Python verifiers
                    (A001220/verify_wieferich.py, A350826/verify_a350826.py) run here
 configs.json       the full-size workloads computed by the oracle (tests/ checks the oracle
@@ -96,6 +97,9 @@ def ref_vectors():
     sec = g.split("## Relation to OEIS A016045", 1)[1].split("\n## ", 1)[0]
     rows = re.findall(r"^\|\s*(\d+)\s*\|\s*(\d+)\s*\|\s*\**([\d,]+)\**", sec, re.M)
     out["A016045"] = [int(v.replace(",", "")) for n, l, v in rows]
+    sec = g.split("## Decreasing gaps: OEIS A263049", 1)[1].split("\n## ", 1)[0]
+    rows = re.findall(r"^\|\s*(\d+)\s*\|\s*(\d+)\s*\|\s*\**([\d,]+)\**", sec, re.M)
+    out["A263049"] = [int(v.replace(",", "")) for n, l, v in rows]
     return out
 
 
