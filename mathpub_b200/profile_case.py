@@ -3,6 +3,7 @@
     python -m mathpub_b200.profile_case sieve  [--lo 1e15] [--log2span 32] [--tile 20] [--threads 1024]
     python -m mathpub_b200.profile_case bpsw   [--log2count 22]
     python -m mathpub_b200.profile_case fermat [--lo 1e12] [--span 1e8]
+    python -m mathpub_b200.profile_case chain  [--lo 1e15] [--span 1e8] [--k 16] [--dec]
 
 The tables are built and every kernel runs once before the profiled region, so the capture
 holds only the steady-state launches of one call.
@@ -23,7 +24,7 @@ def num(s):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("what", choices=["sieve", "bpsw", "fermat"])
+    ap.add_argument("what", choices=["sieve", "bpsw", "fermat", "chain"])
     ap.add_argument("--lo", default="1e15")
     ap.add_argument("--log2span", type=int, default=32)
     ap.add_argument("--span", default="1e8")
@@ -31,6 +32,8 @@ def main():
     ap.add_argument("--threads", type=int, default=0)
     ap.add_argument("--log2count", type=int, default=22)
     ap.add_argument("--plain", action="store_true")
+    ap.add_argument("--k", type=int, default=16)
+    ap.add_argument("--dec", action="store_true")
     a = ap.parse_args()
     import torch
     e = mp.Engine(0)
@@ -43,9 +46,12 @@ def main():
     elif a.what == "bpsw":
         n, _ = mp.bpsw_workload(0x3C0FFEE, 1 << a.log2count, 0)
         run = lambda: e.bpsw(n)
-    else:
+    elif a.what == "fermat":
         lo = num(a.lo)
         run = lambda: e.wieferich_range(lo, lo + num(a.span))
+    else:
+        lo = num(a.lo)
+        run = lambda: e.chain_sieve(lo, lo + num(a.span), a.k, dec=a.dec)
     r0 = run()
     torch.cuda.synchronize()
     torch.cuda.profiler.start()
@@ -55,6 +61,9 @@ def main():
     if a.what == "bpsw":
         assert np.array_equal(r0, r1)
         print("primes", int(r1.sum()))
+    elif a.what == "chain":
+        assert all(np.array_equal(x, y) for x, y in zip(r0, r1))
+        print("chains", len(r1[0]), [(int(h), int(n)) for h, n in zip(*r1)][:8])
     else:
         same = {k: r0[k] for k in r0 if not isinstance(r0[k], np.ndarray)} == \
                {k: r1[k] for k in r1 if not isinstance(r1[k], np.ndarray)}
