@@ -31,9 +31,7 @@
 #include "../../include/gapsieve_cuda.h"
 
 #define CS_K 131072u                          // values of k per class and segment
-#define CS_WORDS (CS_K / 64)
 #define CS_THREADS 256u
-#define CS_WPT (CS_WORDS / CS_THREADS)       // words per thread
 #define CS_MAXG 64                            // pattern groups
 #define CS_SIEVE_LO 1024u                     // mp_chain_sieve: heads below this are checked one by one
 #define CS_PMAX 199u                          // mp_chain_sieve: pattern primes up to this
@@ -160,57 +158,96 @@ struct CsUnit {
     const u32 *bq;                            // [segment][sieve prime]: the segment's base mod q
 };
 
-// one CTA per (class, segment): AND the rotated patterns over the segment's 2^17 values of k
-// and append the survivors' offsets from the unit's base.  Word w = thread + 256 i is coalesced
-// across the warp; a word that is already 0 loads nothing from the later groups.
+// ANDs one group's rotated pattern into a thread's CS_CPT 128-bit chunks.  Chunk c of the class
+// bitmap (bits 128c .. 128c + 127) comes from pattern bits abit + 128c ...: the aligned 16-byte
+// chunks a + c and a + c + 1 (a = abit / 128) joined by four 32-bit funnel shifts; Q =
+// (abit mod 128) / 32 picks the words, s = abit mod 32 the shift.  A chunk with no live bit
+// left loads nothing: at long chains most are dead after the first few groups, which is what
+// keeps the L2 traffic down.
+template <int Q>
+__device__ __forceinline__ void cs_and_group(u32 (&acc)[4][4], const uint4 *__restrict__ pc, u32 s)
+{
+#pragma unroll
+    for (u32 i = 0; i < 4; i++)
+        if (acc[i][0] | acc[i][1] | acc[i][2] | acc[i][3]) {
+            const uint4 X = __ldg(pc + CS_THREADS * i), Y = __ldg(pc + CS_THREADS * i + 1);
+            const u32 x[8] = {X.x, X.y, X.z, X.w, Y.x, Y.y, Y.z, Y.w};
+#pragma unroll
+            for (int w = 0; w < 4; w++) acc[i][w] &= __funnelshift_r(x[w + Q], x[w + Q + 1], s);
+        }
+}
+
+// one CTA per CS_CPB classes of one segment: AND the rotated patterns over each class's 2^17
+// values of k and append the survivors' offsets from the unit's base.  The rotations of all
+// the CTA's classes and groups are taken in parallel before one barrier.
+#define CS_CPB 4u                             // classes per CTA
+#define CS_CPT (CS_K / 128 / CS_THREADS)      // 128-bit chunks per thread and class
+static_assert(CS_CPT == 4, "cs_and_group takes 4 chunks per thread");
 __global__ void __launch_bounds__(CS_THREADS) cs_sieve_kernel(CsTables T, CsShape S, CsUnit U, u64 *list, u64 cap,
                                                               ull *count)
 {
-    __shared__ u32 s_word[CS_MAXG];
-    __shared__ u32 s_sh[CS_MAXG];
-    const u32 j = U.j0 + blockIdx.x % U.nj, g = blockIdx.x / U.nj;
-    const u32 r = S.res[j];
-    const u32 s0 = r >= U.bmodW ? r - U.bmodW : r + U.W - U.bmodW;
+    __shared__ u32 s_chunk[CS_CPB][CS_MAXG];  // first 16-byte chunk of the window
+    __shared__ u32 s_bit[CS_CPB][CS_MAXG];    // bit offset of the window in that chunk
+    __shared__ u32 s_s0[CS_CPB];
+    const u32 nblk = (U.nj + CS_CPB - 1) / CS_CPB;
+    const u32 jb = blockIdx.x % nblk, g = blockIdx.x / nblk;
     const u32 *bq = U.bq + (size_t)g * T.nps;
-    for (u32 gi = threadIdx.x; gi < T.ngroups; gi += CS_THREADS) {
+    for (u32 x = threadIdx.x; x < CS_CPB * T.ngroups; x += CS_THREADS) {
+        const u32 c = x / T.ngroups, gi = x - c * T.ngroups, jj = jb * CS_CPB + c;
+        if (jj >= U.nj) continue;
+        const u32 r = S.res[U.j0 + jj];
+        const u32 s0 = r >= U.bmodW ? r - U.bmodW : r + U.W - U.bmodW;
+        if (gi == 0) s_s0[c] = s0;
         const u32 P = T.ginfo[4 * gi], first = T.ginfo[4 * gi + 1], n = T.ginfo[4 * gi + 2];
         u64 R = 0;
         for (u32 i = first; i < first + n; i++) {
             const u32 q = T.q[i];
             u32 t = bq[i] + s0 % q;
             if (t >= q) t -= q;
-            R += (u64)T.qinv[i] * t % q * T.crt[i];
+            R += (u64)((u64)T.qinv[i] * t % q) * T.crt[i];
         }
-        R %= P;
-        s_word[gi] = T.ginfo[4 * gi + 3] + (u32)(R >> 6);
-        s_sh[gi] = (u32)(R & 63);
+        const u64 abit = 64ull * T.ginfo[4 * gi + 3] + R % P;
+        s_chunk[c][gi] = (u32)(abit >> 7);
+        s_bit[c][gi] = (u32)(abit & 127);
     }
     __syncthreads();
-    u64 acc[CS_WPT];
-#pragma unroll
-    for (u32 i = 0; i < CS_WPT; i++) acc[i] = ~0ull;
-    for (u32 gi = 0; gi < T.ngroups; gi++) {
-        const u64 *pw = S.pat + s_word[gi] + threadIdx.x;
-        const u32 sh = s_sh[gi];
-#pragma unroll
-        for (u32 i = 0; i < CS_WPT; i++)
-            if (acc[i]) {
-                const u64 lo64 = __ldg(pw + CS_THREADS * i), hi64 = __ldg(pw + CS_THREADS * i + 1);
-                acc[i] &= (lo64 >> sh) | ((hi64 << 1) << (63 - sh));   // sh = 0 takes nothing from hi64
-            }
-    }
-    const u64 off0 = (u64)g * U.segsize + s0;
+    const uint4 *pat = (const uint4 *)S.pat;
     const u32 lane = threadIdx.x & 31;
+    for (u32 c = 0; c < CS_CPB; c++) {
+        if (jb * CS_CPB + c >= U.nj) break;                             // uniform
+        u32 acc[4][4];
 #pragma unroll
-    for (u32 i = 0; i < CS_WPT; i++) {
-        u64 m = acc[i];
-        const u64 o0 = off0 + 64ull * (threadIdx.x + CS_THREADS * i) * U.W;
-        if (m && o0 + 63ull * U.W > U.lim) {                           // the unit's end
-            const u64 room = o0 > U.lim ? 0 : (U.lim - o0) / U.W + 1;  // bits 0 .. room - 1 are in range
-            if (room < 64) m &= (1ull << room) - 1;
+        for (u32 i = 0; i < 4; i++)
+#pragma unroll
+            for (u32 w = 0; w < 4; w++) acc[i][w] = ~0u;
+        for (u32 gi = 0; gi < T.ngroups; gi++) {
+            const uint4 *pc = pat + s_chunk[c][gi] + threadIdx.x;
+            const u32 bit = s_bit[c][gi], s = bit & 31;
+            switch (bit >> 5) {                                         // uniform
+            case 0: cs_and_group<0>(acc, pc, s); break;
+            case 1: cs_and_group<1>(acc, pc, s); break;
+            case 2: cs_and_group<2>(acc, pc, s); break;
+            default: cs_and_group<3>(acc, pc, s); break;
+            }
         }
-        const u32 nb = __popcll(m);
-        if (!__ballot_sync(0xffffffffu, nb)) continue;                 // warp-uniform
+        // word w of chunk i holds k = 32 (4 (thread + 256 i) + w) + b
+        const u64 off0 = (u64)g * U.segsize + s_s0[c];
+        if (off0 + (u64)(CS_K - 1) * U.W > U.lim) {                     // the unit's end: offsets <= lim only
+#pragma unroll
+            for (u32 i = 0; i < 4; i++)
+#pragma unroll
+                for (u32 w = 0; w < 4; w++) {
+                    const u64 o0 = off0 + 32ull * (4 * (threadIdx.x + CS_THREADS * i) + w) * U.W;
+                    const u64 room = o0 > U.lim ? 0 : (U.lim - o0) / U.W + 1;
+                    if (room < 32) acc[i][w] &= (1u << room) - 1;
+                }
+        }
+        u32 nb = 0;
+#pragma unroll
+        for (u32 i = 0; i < 4; i++)
+#pragma unroll
+            for (u32 w = 0; w < 4; w++) nb += __popc(acc[i][w]);
+        if (!__ballot_sync(0xffffffffu, nb)) continue;                  // warp-uniform
         u32 incl = nb;
 #pragma unroll
         for (int d = 1; d < 32; d <<= 1) {
@@ -222,12 +259,20 @@ __global__ void __launch_bounds__(CS_THREADS) cs_sieve_kernel(CsTables T, CsShap
         if (lane == 31) bpos = atomicAdd(count, (ull)tot);
         bpos = __shfl_sync(0xffffffffu, bpos, 31);
         u64 pos = bpos + incl - nb;
-        while (m) {
-            const u32 b = __ffsll((long long)m) - 1;
-            m &= m - 1;
-            if (pos < cap) list[pos] = o0 + (u64)b * U.W;
-            pos++;
-        }
+        if (!nb) continue;
+#pragma unroll
+        for (u32 i = 0; i < 4; i++)
+#pragma unroll
+            for (u32 w = 0; w < 4; w++) {
+                u32 m = acc[i][w];
+                const u64 o0 = off0 + 32ull * (4 * (threadIdx.x + CS_THREADS * i) + w) * U.W;
+                while (m) {
+                    const u32 b = __ffs(m) - 1;
+                    m &= m - 1;
+                    if (pos < cap) list[pos] = o0 + (u64)b * U.W;
+                    pos++;
+                }
+            }
     }
 }
 
@@ -335,7 +380,7 @@ static void cs_queue_unit(const CsTables &T, const CsShape &S, const CsUnit &U, 
 {
     const u32 rounds = std::min(split, S.k);
     cudaMemsetAsync(L.cnt, 0, (size_t)(rounds + 2) * sizeof(ull), st);
-    cs_sieve_kernel<<<U.nj * U.nseg, CS_THREADS, 0, st>>>(T, S, U, L.list[0], L.cap, L.cnt);
+    cs_sieve_kernel<<<(U.nj + CS_CPB - 1) / CS_CPB * U.nseg, CS_THREADS, 0, st>>>(T, S, U, L.list[0], L.cap, L.cnt);
     const unsigned grid = (unsigned)sm_count * 8;
     int cur = 0;
     for (u32 r = 0; r < rounds; r++, cur ^= 1)
@@ -500,6 +545,12 @@ struct ChainDev {
     u32 k = 0, shape = 0;
     bool ok = false;                           // false: no chain of this shape and length above CS_SIEVE_LO
     CsPlan plan;
+    // the last result when the caller's arrays were too small, for the call that follows with
+    // room for all of it (count first, then fill) so that the range is not sieved twice
+    bool kept = false;
+    u64 kept_lo = 0, kept_hi = 0;
+    std::vector<u64> kept_h;
+    std::vector<u32> kept_l;
     DevBuf ginfo, q, qinv, crt, pat, res, offs, bq, l0, l1, cnt, rh, rl;
     void release()
     {
@@ -577,6 +628,15 @@ extern "C" int mp_chain_sieve(mp_handle *h, uint64_t lo, uint64_t hi, uint32_t k
     }
     ChainDev &D = *h->chain;
     const CsPlan &P = D.plan;
+    if (D.kept && D.kept_lo == lo && D.kept_hi == hi) {
+        const size_t m = std::min(cap, D.kept_h.size());
+        std::copy(D.kept_h.begin(), D.kept_h.begin() + m, heads);
+        std::copy(D.kept_l.begin(), D.kept_l.begin() + m, lens);
+        *count = D.kept_h.size();
+        if (m == D.kept_h.size()) { D.kept = false; D.kept_h = {}; D.kept_l = {}; }
+        return MP_OK;
+    }
+    D.kept = false;
     std::vector<u64> H;
     std::vector<u32> L;
     // heads below CS_SIEVE_LO (where a member may be a sieve prime): every odd p, exactly
@@ -639,6 +699,13 @@ extern "C" int mp_chain_sieve(mp_handle *h, uint64_t lo, uint64_t hi, uint32_t k
     std::copy(H.begin(), H.begin() + m, heads);
     std::copy(L.begin(), L.begin() + m, lens);
     *count = H.size();
+    if (m < H.size()) {
+        D.kept = true;
+        D.kept_lo = lo;
+        D.kept_hi = hi;
+        D.kept_h.swap(H);
+        D.kept_l.swap(L);
+    }
     return MP_OK;
 }
 

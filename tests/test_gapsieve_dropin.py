@@ -74,12 +74,18 @@ def test_sprp_batch_matches_python():
     assert [bool(x) for x in ok] == [sprp2(n) for n in ns]
 
 
-def run(exe, args):
+def run(exe, args, log=None):
     p = os.path.join(REF, exe)
     if not os.path.exists(p):
         pytest.skip(f"oracle/_ref/{exe} is not built")
-    r = subprocess.run([p, *args.split(), "-q"], capture_output=True, text=True, timeout=900)
+    extra = ["--log", str(log)] if log else []
+    r = subprocess.run([p, *args.split(), "-q", *extra], capture_output=True, text=True, timeout=900)
     assert r.returncode == 0, r.stderr[-600:]
+    # the host redoes a failed GPU unit and then searches it on the CPU (exactly), which would
+    # hide a GPU failure from the comparison; the GPU must have done every unit
+    assert "on the CPU" not in r.stderr
+    if log:
+        assert "failed" not in open(log).read()
     # the summary: counts by length, or the --first answer; without the header line (it names
     # the CPU threads or the GPU), the progress line and durations
     summary = [re.sub(r"\d+:\d\d:\d\d", "", line) for line in r.stderr.splitlines()
@@ -96,9 +102,9 @@ def run(exe, args):
     "-l 10 -g both -s 100000000000000000000 -e 100000010000000000000",
     "-l 15 -s 221860000000000000 -e 221870000000000000 --first",
 ])
-def test_reference_gapsieve_on_the_gpu_matches_its_cpu_build(args):
+def test_reference_gapsieve_on_the_gpu_matches_its_cpu_build(args, tmp_path):
     cpu_lines, cpu_counts = run("gapsieve_cpu", args)
-    gpu_lines, gpu_counts = run("gapsieve_gpu", args + " -t 0 --gpu")
+    gpu_lines, gpu_counts = run("gapsieve_gpu", args + " -t 0 --gpu", log=tmp_path / "gpu.log")
     assert len(cpu_lines) > 0
     assert gpu_lines == cpu_lines
     assert gpu_counts == cpu_counts
