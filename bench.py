@@ -289,6 +289,7 @@ def run_ours(args):
     hbm, hbm_src = peaks_file()
 
     fermat = run_fermat(e, world, rank, dev) if not args.quick else None
+    chains = run_chains(e) if (rank == 0 and not args.quick) else None
     serving = run_serving(e, args) if (rank == 0 and not args.quick and args.serve_requests) else None
 
     line = None
@@ -348,6 +349,7 @@ def run_ours(args):
                      "workload": "2^26 seeded odd u64 (60% uniform [2^40,2^64), 30% p*q near 2^62, "
                                  "10% (k+1)(2k+1) / Chernick), 4096 lists, log-uniform lengths"},
             "fermat": fermat,
+            "chains": chains,
             "serving": serving,
             "autotune": tune_report.strip().splitlines()[-3:] if tune_report != "off" else "off",
             "probes": peaks,
@@ -390,6 +392,26 @@ def run_fermat(e, world, rank, dev):
             "e2e_tests_per_s": r["tests"] / wall, "e2e_ms": wall * 1e3, "near": r["near"], "flt": r["flt"],
             "cks": r["cks"], "results_match_fixture": fix,
             "job": {k: job[k] for k in ("primes", "tests", "near", "flt", "cks", "ordered_hash", "nhits")} if job else None}
+
+
+CHAIN_A15 = 1397398433200922807          # A016045 a(15): 16 primes with gaps 2, 4, ..., 30
+CHAIN_SPAN = 2 * 10 ** 16
+
+
+def run_chains(e):
+    """The constellation sieve (mp_chain_sieve): chains of 16 consecutive primes with gaps 2,
+    4, ..., 30 in [a15 - 1e16, a15 + 1e16), a15 = A016045 a(15); wall time of the host call
+    (it synchronises), after a warm-up call that builds the wheel and patterns for k = 16."""
+    lo = CHAIN_A15 - CHAIN_SPAN // 2
+    e.chain_sieve(lo, lo + 10 ** 13, 16)
+    t0 = time.perf_counter()
+    heads, lens = e.chain_sieve(lo, lo + CHAIN_SPAN, 16)
+    wall = time.perf_counter() - t0
+    found = [(int(h), int(n)) for h, n in zip(heads, lens)]
+    return {"workload": "chains of >= 16 consecutive primes with gaps 2, 4, ..., 30 in [a15 - 1e16, a15 + 1e16), "
+                        "a15 = A016045 a(15) = 1397398433200922807",
+            "value": CHAIN_SPAN / wall, "unit": "integers/s", "ms": wall * 1e3, "chains": found,
+            "finds_a15": (CHAIN_A15, 16) in found}
 
 
 def run_serving(e, args):
@@ -518,6 +540,17 @@ def cpu_baseline(sample_log2=31):
         t0 = time.perf_counter()
         oracle.ref_count_sext(lo, hi, t)
         dt = time.perf_counter() - t0
+        gs = os.path.join(ROOT, "oracle", "_ref", "gapsieve_cpu")
+        if os.path.exists(gs):
+            clo = CHAIN_A15 - 10 ** 14
+            t0 = time.perf_counter()
+            r = subprocess.run([gs, "-l", "16", "-s", str(clo), "-e", str(clo + 2 * 10 ** 14 - 1), "-q",
+                                "-t", str(t)], capture_output=True, text=True)
+            dt = time.perf_counter() - t0
+            if r.returncode == 0:
+                out["chains"] = {"value": 2e14 / dt, "unit": "integers/s", "cores": t, "kind": "reference",
+                                 "sample": f"gapchain/gapsieve.c (its CPU build) -l 16 over [a15 - 1e14, a15 + 1e14), "
+                                           f"{t} threads, {dt:.2f} s"}
         out["reference_sextuplet_count"] = {"value": (hi - lo) / dt, "unit": "ints/s", "kind": "reference",
                                             "sample": f"a350826 count [1e15, 1e15+2^{sample_log2}), {t} threads "
                                                       "(6-tuples only: it sieves the admissible classes, not all "
