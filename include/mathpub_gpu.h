@@ -174,6 +174,18 @@ int mp_gap_chains(mp_handle *h, uint64_t lo, uint64_t hi, uint32_t min_len, uint
 int mp_chain_sieve(mp_handle *h, uint64_t lo, uint64_t hi, uint32_t k, uint32_t shape, uint64_t *heads,
                    uint32_t *lens, size_t cap, size_t *count);
 
+/* a prime constellation by the same sieve: *count = the number of p in [lo, hi) with p + offs[i]
+ * prime for every i (members may lie beyond hi), *cks = the sum of mix64(p) mod 2^64 over them.
+ * offs[0] = 0 < offs[1] < ... < offs[k-1] <= MP_TUPLE_MAXOFF, all even, 2 <= k <= MP_TUPLE_MAXK,
+ * hi <= MP_CHAIN_SIEVE_HI_MAX.  With offs = {0, 4, 6, 10, 12, 16} it counts the prime sextuplets
+ * of A350826 as that program's class sieve does (process_class A350826/a350826.c:1522, the
+ * count and checksum of found :1364-1379): the same count and checksum as mp_sieve_range's
+ * tuple6 and tuple6_cks, from a search that sieves the admissible classes only. */
+#define MP_TUPLE_MAXK 64
+#define MP_TUPLE_MAXOFF 2048
+int mp_tuple_count(mp_handle *h, uint64_t lo, uint64_t hi, const uint32_t *offs, uint32_t k, uint64_t *count,
+                   uint64_t *cks);
+
 /* ---- BPSW ----
  * verdict bit i (bit i & 7 of byte i >> 3) = 1 iff n[i] is prime.  For n < 2^64 this is
  * BPSW (base-2 strong test + strong Lucas test with Selfridge's parameters) after trial

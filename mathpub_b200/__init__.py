@@ -118,6 +118,7 @@ def lib():
             "mp_gap_stats_range": ([vp, u64, u64, vp], C.c_int),
             "mp_gap_chains": ([vp, u64, u64, u32, vp, vp, C.c_size_t, C.POINTER(C.c_size_t)], C.c_int),
             "mp_chain_sieve": ([vp, u64, u64, u32, u32, vp, vp, C.c_size_t, C.POINTER(C.c_size_t)], C.c_int),
+            "mp_tuple_count": ([vp, u64, u64, vp, u32, C.POINTER(u64), C.POINTER(u64)], C.c_int),
             "mp_autotune": ([vp, u64, C.c_char_p, C.c_size_t], C.c_int),
             "mp_profile_enable": ([vp, C.c_int], C.c_int),
             "mp_profile_read": ([vp, vp, vp, C.c_int], C.c_int),
@@ -286,6 +287,14 @@ class Engine:
         lens = np.zeros(max(1, n.value), dtype=np.uint32)
         self._check(lib().mp_chain_sieve(self._h, lo, hi, k, shape, _p(heads), _p(lens), n.value, C.byref(n)))
         return heads[:n.value], lens[:n.value]
+
+    def tuple_count(self, lo, hi, offs):
+        """(count, checksum) of the p in [lo, hi) with p + o prime for every o in offs
+        (mp_tuple_count; offs starts at 0, even and increasing)."""
+        o = np.ascontiguousarray(offs, dtype=np.uint32)
+        n, c = C.c_uint64(), C.c_uint64()
+        self._check(lib().mp_tuple_count(self._h, lo, hi, _p(o), len(o), C.byref(n), C.byref(c)))
+        return n.value, c.value
 
     def wieferich_range(self, lo, hi):
         out = WiefStats()

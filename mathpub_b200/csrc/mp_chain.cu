@@ -421,23 +421,29 @@ bool is_small_prime(u32 q)
 }
 
 struct CsPlan {
-    u32 k = 0, shape = 0;
+    u32 k = 0;
     u64 W = 1;
     std::vector<u32> res, offs, ginfo, q, qinv, crt;
     std::vector<u64> pat;
     double survive = 1;                         // the fraction of k values the patterns keep
 };
 
-// the wheel (grown while W <= 3e7 and the classes number at most 24,000), the pattern groups
-// of the primes above it up to CS_PMAX (periods up to 2^24) and their patterns.  False when
-// some prime leaves no admissible residue: then no chain of this shape and length has a head
-// at or above CS_SIEVE_LO.
-bool make_plan(u32 k, u32 shape, CsPlan &P)
+// member offsets of a chain of k primes: gaps 2, 4, ... (shape 0) or ..., 4, 2 (shape 1)
+std::vector<u32> chain_offsets(u32 k, u32 shape)
 {
-    P.k = k;
-    P.shape = shape;
-    P.offs.resize(k);
-    for (u32 m = 0; m < k; m++) P.offs[m] = shape == 0 ? m * (m + 1) : m * (2 * k - 1 - m);
+    std::vector<u32> o(k);
+    for (u32 m = 0; m < k; m++) o[m] = shape == 0 ? m * (m + 1) : m * (2 * k - 1 - m);
+    return o;
+}
+
+// for the member offsets offs: the wheel (grown while W <= 3e7 and the classes number at most
+// 24,000), the pattern groups of the primes above it up to CS_PMAX (periods up to 2^24) and
+// their patterns.  False when some prime leaves no admissible residue: then no p at or above
+// CS_SIEVE_LO has all its members prime.
+bool make_plan(const std::vector<u32> &offs, CsPlan &P)
+{
+    P.k = (u32)offs.size();
+    P.offs = offs;
     std::vector<u64> cls{0};
     u64 W = 1;
     u32 q = 2;
@@ -539,14 +545,34 @@ template <class T> cudaError_t upload(DevBuf &b, const std::vector<T> &v)
 
 }  // namespace
 
-// ---- mp_chain_sieve ----
+// exact check of the screen's survivors for mp_tuple_count: every member prime; count and sum
+// of mix64(p) into the two counters
+__global__ void __launch_bounds__(128) cs_tuple_kernel(const u64 *__restrict__ in, const ull *nin, u64 cap, u64 base,
+                                                       const u32 *__restrict__ offs, u32 k, ull *acc)
+{
+    const u64 n = min((u64)*nin, cap);
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
+        const u64 p = base + in[i];
+        bool ok = true;
+        for (u32 m = 0; m < k && ok; m++) ok = is_prime_exact(p + offs[m]);
+        if (ok) {
+            atomicAdd(acc, 1ull);
+            atomicAdd(acc + 1, (ull)mp_mix64(p));
+        }
+    }
+}
+
+// ---- mp_chain_sieve and mp_tuple_count: one plan and one set of buffers per handle ----
+
+#define CS_MODE_TUPLE 2u                       // modes 0 and 1 are the chain shapes
 
 struct ChainDev {
-    u32 k = 0, shape = 0;
-    bool ok = false;                           // false: no chain of this shape and length above CS_SIEVE_LO
+    u32 mode = 0, k = 0;
+    std::vector<u32> key;                      // the member offsets the plan was built for
+    bool ok = false;                           // false: no admissible p at or above CS_SIEVE_LO
     CsPlan plan;
-    // the last result when the caller's arrays were too small, for the call that follows with
-    // room for all of it (count first, then fill) so that the range is not sieved twice
+    // the last chain list when the caller's arrays were too small, for the call that follows
+    // with room for all of it (count first, then fill) so that the range is not sieved twice
     bool kept = false;
     u64 kept_lo = 0, kept_hi = 0;
     std::vector<u64> kept_h;
@@ -557,6 +583,10 @@ struct ChainDev {
         for (DevBuf *b : {&ginfo, &q, &qinv, &crt, &pat, &res, &offs, &bq, &l0, &l1, &cnt, &rh, &rl}) b->release();
     }
 };
+// counters in D.cnt: CS_NCNT for the unit's lists, then the chain count, then the tuple count
+// and checksum
+#define CS_CNT_RES CS_NCNT
+#define CS_CNT_TUPLE (CS_NCNT + 1)
 
 void mp_chain_free(mp_handle *h)
 {
@@ -566,16 +596,104 @@ void mp_chain_free(mp_handle *h)
     h->chain = nullptr;
 }
 
+// the handle's plan for (mode, offs), built and uploaded when it differs from the last one
+static int cs_prepare(mp_handle *h, u32 mode, const std::vector<u32> &offs)
+{
+    if (h->chain && h->chain->mode == mode && h->chain->key == offs) return MP_OK;
+    mp_chain_free(h);
+    h->chain = new ChainDev();
+    ChainDev &D = *h->chain;
+    D.mode = mode;
+    D.k = (u32)offs.size();
+    D.key = offs;
+    D.ok = make_plan(offs, D.plan);
+    const CsPlan &P = D.plan;
+    if (D.ok) {
+        MP_CUDA(h, upload(D.ginfo, P.ginfo));
+        MP_CUDA(h, upload(D.q, P.q));
+        MP_CUDA(h, upload(D.qinv, P.qinv));
+        MP_CUDA(h, upload(D.crt, P.crt));
+        MP_CUDA(h, upload(D.pat, P.pat));
+        MP_CUDA(h, upload(D.res, P.res));
+    }
+    MP_CUDA(h, upload(D.offs, P.offs));
+    MP_CUDA(h, D.cnt.ensure((CS_NCNT + 3) * sizeof(ull)));
+    return MP_OK;
+}
+
+// every candidate of [lo, hi): the odd p below CS_SIEVE_LO (where a member may be a sieve
+// prime) as one list, then the sieve's units; collect(list, count on the device, capacity,
+// base, expected survivors) checks each list exactly
+template <class Collect>
+static int cs_sieve_range(mp_handle *h, ChainDev &D, u64 lo, u64 hi, cudaStream_t st, Collect &&collect)
+{
+    const CsPlan &P = D.plan;
+    if (lo < CS_SIEVE_LO) {
+        std::vector<u64> strip;
+        for (u64 p = std::max<u64>(lo, 3) | 1; p < std::min<u64>(hi, CS_SIEVE_LO); p += 2) strip.push_back(p);
+        if (!strip.empty()) {
+            MP_CUDA(h, upload(D.l0, strip));
+            const ull n = strip.size();
+            MP_CUDA(h, cudaMemcpy(D.cnt.p, &n, sizeof n, cudaMemcpyHostToDevice));
+            MP_TRY(collect(D.l0.as<u64>(), D.cnt.as<ull>(), n, (u64)0, n));
+        }
+    }
+    const u64 slo = std::max<u64>(lo, CS_SIEVE_LO);
+    if (!D.ok || slo >= hi) return MP_OK;
+    const u64 W = P.W, segsize = (u64)CS_K * W;
+    const u32 A = (u32)P.res.size(), nps = (u32)P.q.size();
+    const u64 nseg_all = (hi - slo + segsize - 1) / segsize;
+    // units: runs of segments (or, for dense patterns, runs of classes of one segment) sized
+    // for about 2^24 expected sieve survivors
+    const double per_class = (double)CS_K * P.survive, target = 16777216.0;
+    u32 useg = 1, ucls = A;
+    if (per_class * A <= target) useg = (u32)std::min<double>(256.0, std::floor(target / (per_class * A)));
+    else ucls = (u32)std::max<double>(1.0, std::floor(target / per_class));
+    u64 ucap = (u64)(1.25 * per_class * ucls * useg) + 65536;
+    const CsTables T{D.ginfo.as<u32>(), D.q.as<u32>(), D.qinv.as<u32>(), D.crt.as<u32>(), (u32)(P.ginfo.size() / 4),
+                     nps};
+    const CsShape S{D.pat.as<u64>(), D.res.as<u32>(), D.offs.as<u32>(), A, D.k};
+    std::vector<u32> bq((size_t)useg * nps);
+    MP_CUDA(h, D.bq.ensure(bq.size() * 4));
+    for (u64 s = 0; s < nseg_all; s += useg) {
+        const u32 ns = (u32)std::min<u64>(useg, nseg_all - s);
+        const u64 base = slo + s * segsize;
+        for (u32 g = 0; g < ns; g++)
+            for (u32 i = 0; i < nps; i++) bq[(size_t)g * nps + i] = (u32)((base + g * segsize) % P.q[i]);
+        MP_CUDA(h, cudaMemcpyAsync(D.bq.p, bq.data(), (size_t)ns * nps * 4, cudaMemcpyHostToDevice, st));
+        for (u32 j0 = 0; j0 < A; j0 += ucls) {
+            const CsUnit U{base, 0, hi - 1 - base, segsize, (u32)W, (u32)(base % W), ns, j0, std::min(ucls, A - j0),
+                           D.bq.as<u32>()};
+            for (;;) {
+                MP_CUDA(h, D.l0.ensure(ucap * 8));
+                MP_CUDA(h, D.l1.ensure(ucap * 8));
+                const CsLists Ls{{D.l0.as<u64>(), D.l1.as<u64>()}, ucap, D.cnt.as<ull>()};
+                int fin = 0;
+                u32 fcnt = 0;
+                cs_queue_unit(T, S, U, Ls, 3, h->sm_count, st, &fin, &fcnt);
+                MP_CUDA(h, cudaGetLastError());
+                ull raw = 0;
+                MP_CUDA(h, cudaMemcpyAsync(&raw, D.cnt.p, sizeof raw, cudaMemcpyDeviceToHost, st));
+                MP_CUDA(h, cudaStreamSynchronize(st));
+                if (raw > ucap) { ucap = raw + raw / 4 + 65536; continue; }       // lists overflowed: again
+                MP_TRY(collect(Ls.list[fin], D.cnt.as<ull>() + fcnt, ucap, base, raw / 8 + 1));
+                break;
+            }
+        }
+    }
+    return MP_OK;
+}
+
 // verify a survivor list (offsets from base, count on the device) and append the chains
 static int cs_collect(mp_handle *h, ChainDev &D, const u64 *list, const ull *nin, u64 cap, u64 base, u64 expect,
                       std::vector<u64> &H, std::vector<u32> &L, cudaStream_t st)
 {
-    ull *nres = D.cnt.as<ull>() + CS_NCNT;
+    ull *nres = D.cnt.as<ull>() + CS_CNT_RES;
     MP_CUDA(h, D.rh.ensure(cap * 8));
     MP_CUDA(h, D.rl.ensure(cap * 4));
     MP_CUDA(h, cudaMemsetAsync(nres, 0, sizeof(ull), st));
     const u64 grid = std::max<u64>(1, std::min<u64>((expect + 127) / 128, (u64)h->sm_count * 16));
-    cs_verify_kernel<<<(unsigned)grid, 128, 0, st>>>(list, nin, cap, base, D.k, D.shape, D.rh.as<u64>(), D.rl.as<u32>(),
+    cs_verify_kernel<<<(unsigned)grid, 128, 0, st>>>(list, nin, cap, base, D.k, D.mode, D.rh.as<u64>(), D.rl.as<u32>(),
                                                      nres);
     MP_CUDA(h, cudaGetLastError());
     ull nr = 0;
@@ -607,27 +725,8 @@ extern "C" int mp_chain_sieve(mp_handle *h, uint64_t lo, uint64_t hi, uint32_t k
     std::lock_guard<std::recursive_mutex> lk(h->mu);
     MP_CUDA(h, cudaSetDevice(h->device));
     cudaStream_t st = h->stream;
-    if (!h->chain || h->chain->k != k || h->chain->shape != shape) {
-        mp_chain_free(h);
-        h->chain = new ChainDev();
-        ChainDev &D = *h->chain;
-        D.k = k;
-        D.shape = shape;
-        D.ok = make_plan(k, shape, D.plan);
-        const CsPlan &P = D.plan;
-        if (D.ok) {
-            MP_CUDA(h, upload(D.ginfo, P.ginfo));
-            MP_CUDA(h, upload(D.q, P.q));
-            MP_CUDA(h, upload(D.qinv, P.qinv));
-            MP_CUDA(h, upload(D.crt, P.crt));
-            MP_CUDA(h, upload(D.pat, P.pat));
-            MP_CUDA(h, upload(D.res, P.res));
-        }
-        MP_CUDA(h, upload(D.offs, P.offs));
-        MP_CUDA(h, D.cnt.ensure((CS_NCNT + 1) * sizeof(ull)));
-    }
+    MP_TRY(cs_prepare(h, shape, chain_offsets(k, shape)));
     ChainDev &D = *h->chain;
-    const CsPlan &P = D.plan;
     if (D.kept && D.kept_lo == lo && D.kept_hi == hi) {
         const size_t m = std::min(cap, D.kept_h.size());
         std::copy(D.kept_h.begin(), D.kept_h.begin() + m, heads);
@@ -639,61 +738,9 @@ extern "C" int mp_chain_sieve(mp_handle *h, uint64_t lo, uint64_t hi, uint32_t k
     D.kept = false;
     std::vector<u64> H;
     std::vector<u32> L;
-    // heads below CS_SIEVE_LO (where a member may be a sieve prime): every odd p, exactly
-    if (lo < CS_SIEVE_LO) {
-        std::vector<u64> strip;
-        for (u64 p = std::max<u64>(lo, 3) | 1; p < std::min<u64>(hi, CS_SIEVE_LO); p += 2) strip.push_back(p);
-        if (!strip.empty()) {
-            MP_CUDA(h, upload(D.l0, strip));
-            const ull n = strip.size();
-            MP_CUDA(h, cudaMemcpy(D.cnt.p, &n, sizeof n, cudaMemcpyHostToDevice));
-            MP_TRY(cs_collect(h, D, D.l0.as<u64>(), D.cnt.as<ull>(), n, 0, n, H, L, st));
-        }
-    }
-    const u64 slo = std::max<u64>(lo, CS_SIEVE_LO);
-    if (D.ok && slo < hi) {
-        const u64 W = P.W, segsize = (u64)CS_K * W;
-        const u32 A = (u32)P.res.size(), nps = (u32)P.q.size();
-        const u64 nseg_all = (hi - slo + segsize - 1) / segsize;
-        // units: runs of segments (or, for short chains, runs of classes of one segment) sized
-        // for about 2^24 expected sieve survivors
-        const double per_class = (double)CS_K * P.survive, target = 16777216.0;
-        u32 useg = 1, ucls = A;
-        if (per_class * A <= target) useg = (u32)std::min<double>(256.0, std::floor(target / (per_class * A)));
-        else ucls = (u32)std::max<double>(1.0, std::floor(target / per_class));
-        u64 ucap = (u64)(1.25 * per_class * ucls * useg) + 65536;
-        const CsTables T{D.ginfo.as<u32>(), D.q.as<u32>(), D.qinv.as<u32>(), D.crt.as<u32>(),
-                         (u32)(P.ginfo.size() / 4), nps};
-        const CsShape S{D.pat.as<u64>(), D.res.as<u32>(), D.offs.as<u32>(), A, k};
-        std::vector<u32> bq((size_t)useg * nps);
-        MP_CUDA(h, D.bq.ensure(bq.size() * 4));
-        for (u64 s = 0; s < nseg_all; s += useg) {
-            const u32 ns = (u32)std::min<u64>(useg, nseg_all - s);
-            const u64 base = slo + s * segsize;
-            for (u32 g = 0; g < ns; g++)
-                for (u32 i = 0; i < nps; i++) bq[(size_t)g * nps + i] = (u32)((base + g * segsize) % P.q[i]);
-            MP_CUDA(h, cudaMemcpyAsync(D.bq.p, bq.data(), (size_t)ns * nps * 4, cudaMemcpyHostToDevice, st));
-            for (u32 j0 = 0; j0 < A; j0 += ucls) {
-                const CsUnit U{base, 0, hi - 1 - base, segsize, (u32)W, (u32)(base % W), ns, j0,
-                               std::min(ucls, A - j0), D.bq.as<u32>()};
-                for (;;) {
-                    MP_CUDA(h, D.l0.ensure(ucap * 8));
-                    MP_CUDA(h, D.l1.ensure(ucap * 8));
-                    const CsLists Ls{{D.l0.as<u64>(), D.l1.as<u64>()}, ucap, D.cnt.as<ull>()};
-                    int fin = 0;
-                    u32 fcnt = 0;
-                    cs_queue_unit(T, S, U, Ls, 3, h->sm_count, st, &fin, &fcnt);
-                    MP_CUDA(h, cudaGetLastError());
-                    ull raw = 0;
-                    MP_CUDA(h, cudaMemcpyAsync(&raw, D.cnt.p, sizeof raw, cudaMemcpyDeviceToHost, st));
-                    MP_CUDA(h, cudaStreamSynchronize(st));
-                    if (raw > ucap) { ucap = raw + raw / 4 + 65536; continue; }   // lists overflowed: again
-                    MP_TRY(cs_collect(h, D, Ls.list[fin], D.cnt.as<ull>() + fcnt, ucap, base, raw / 8 + 1, H, L, st));
-                    break;
-                }
-            }
-        }
-    }
+    MP_TRY(cs_sieve_range(h, D, lo, hi, st, [&](const u64 *list, const ull *nin, u64 cap_, u64 base, u64 expect) {
+        return cs_collect(h, D, list, nin, cap_, base, expect, H, L, st);
+    }));
     sort_chains(H, L);
     const size_t m = std::min(cap, H.size());
     std::copy(H.begin(), H.begin() + m, heads);
@@ -706,6 +753,39 @@ extern "C" int mp_chain_sieve(mp_handle *h, uint64_t lo, uint64_t hi, uint32_t k
         D.kept_h.swap(H);
         D.kept_l.swap(L);
     }
+    return MP_OK;
+}
+
+extern "C" int mp_tuple_count(mp_handle *h, uint64_t lo, uint64_t hi, const uint32_t *offs, uint32_t k,
+                              uint64_t *count, uint64_t *cks)
+{
+    if (!h || !offs || !count || !cks) return MP_EINVAL;
+    *count = 0;
+    *cks = 0;
+    if (k < 2 || k > MP_TUPLE_MAXK) return mp_set_error(h, MP_EINVAL, "k must be in 2..%d", MP_TUPLE_MAXK);
+    if (offs[0] != 0) return mp_set_error(h, MP_EINVAL, "offs[0] must be 0");
+    for (u32 i = 1; i < k; i++)
+        if (offs[i] <= offs[i - 1] || (offs[i] & 1) || offs[i] > MP_TUPLE_MAXOFF)
+            return mp_set_error(h, MP_EINVAL, "offsets must be even and increasing, at most %d", MP_TUPLE_MAXOFF);
+    if (hi > MP_CHAIN_SIEVE_HI_MAX) return mp_set_error(h, MP_ERANGE, "hi must be <= 2^64 - 2^12");
+    if (hi <= lo) return MP_OK;
+    std::lock_guard<std::recursive_mutex> lk(h->mu);
+    MP_CUDA(h, cudaSetDevice(h->device));
+    cudaStream_t st = h->stream;
+    MP_TRY(cs_prepare(h, CS_MODE_TUPLE, std::vector<u32>(offs, offs + k)));
+    ChainDev &D = *h->chain;
+    ull *acc = D.cnt.as<ull>() + CS_CNT_TUPLE;
+    MP_CUDA(h, cudaMemsetAsync(acc, 0, 2 * sizeof(ull), st));
+    MP_TRY(cs_sieve_range(h, D, lo, hi, st, [&](const u64 *list, const ull *nin, u64 cap_, u64 base, u64 expect) {
+        const u64 grid = std::max<u64>(1, std::min<u64>((expect + 127) / 128, (u64)h->sm_count * 16));
+        cs_tuple_kernel<<<(unsigned)grid, 128, 0, st>>>(list, nin, cap_, base, D.offs.as<u32>(), D.k, acc);
+        return cudaGetLastError() == cudaSuccess ? MP_OK : mp_set_error(h, MP_ECUDA, "tuple kernel launch failed");
+    }));
+    ull r[2] = {0, 0};
+    MP_CUDA(h, cudaMemcpyAsync(r, acc, sizeof r, cudaMemcpyDeviceToHost, st));
+    MP_CUDA(h, cudaStreamSynchronize(st));
+    *count = r[0];
+    *cks = r[1];
     return MP_OK;
 }
 
