@@ -290,6 +290,7 @@ def run_ours(args):
 
     fermat = run_fermat(e, world, rank, dev) if not args.quick else None
     chains = run_chains(e) if (rank == 0 and not args.quick) else None
+    tuples = run_tuples(e) if (rank == 0 and not args.quick) else None
     serving = run_serving(e, args) if (rank == 0 and not args.quick and args.serve_requests) else None
 
     line = None
@@ -350,6 +351,7 @@ def run_ours(args):
                                  "10% (k+1)(2k+1) / Chernick), 4096 lists, log-uniform lengths"},
             "fermat": fermat,
             "chains": chains,
+            "tuples": tuples,
             "serving": serving,
             "autotune": tune_report.strip().splitlines()[-3:] if tune_report != "off" else "off",
             "probes": peaks,
@@ -412,6 +414,32 @@ def run_chains(e):
                         "a15 = A016045 a(15) = 1397398433200922807",
             "value": CHAIN_SPAN / wall, "unit": "integers/s", "ms": wall * 1e3, "chains": found,
             "finds_a15": (CHAIN_A15, 16) in found}
+
+
+SEXTUPLET = [0, 4, 6, 10, 12, 16]
+
+
+def run_tuples(e):
+    """Prime sextuplets p + {0, 4, 6, 10, 12, 16} in [1e15, 1e15 + 2e12) by the constellation
+    sieve (mp_tuple_count, admissible classes only), against the reference's window of that
+    range (count and checksum); best of three host calls after a warm-up."""
+    lo, hi = 10 ** 15, 10 ** 15 + 2 * 10 ** 12
+    e.tuple_count(lo, lo + 10 ** 11, SEXTUPLET)
+    best, res = None, None
+    for _ in range(3):
+        t0 = time.perf_counter()
+        res = e.tuple_count(lo, hi, SEXTUPLET)
+        dt = time.perf_counter() - t0
+        best = dt if best is None else min(best, dt)
+    fix = None
+    try:
+        with open(os.path.join(ROOT, "tests", "golden", "ref_vectors.json")) as f:
+            w = json.load(f)["sext_windows"][0]
+        fix = (w["lo"], w["hi"], w["count"], w["cks"]) == ("1e15", "1e15+2e12", res[0], res[1])
+    except Exception:
+        pass
+    return {"workload": "prime sextuplets p + {0,4,6,10,12,16}, p in [1e15, 1e15+2e12)", "value": (hi - lo) / best,
+            "unit": "integers/s", "ms": best * 1e3, "count": res[0], "cks": res[1], "matches_reference_window": fix}
 
 
 def run_serving(e, args):
