@@ -74,12 +74,13 @@ def test_sprp_batch_matches_python():
     assert [bool(x) for x in ok] == [sprp2(n) for n in ns]
 
 
-def run(exe, args, log=None):
+def run(exe, args, log=None, env=None):
     p = os.path.join(REF, exe)
     if not os.path.exists(p):
         pytest.skip(f"oracle/_ref/{exe} is not built")
     extra = ["--log", str(log)] if log else []
-    r = subprocess.run([p, *args.split(), "-q", *extra], capture_output=True, text=True, timeout=900)
+    r = subprocess.run([p, *args.split(), "-q", *extra], capture_output=True, text=True, timeout=900,
+                       env={**os.environ, **(env or {})})
     assert r.returncode == 0, r.stderr[-600:]
     # the host redoes a failed GPU unit and then searches it on the CPU (exactly), which would
     # hide a GPU failure from the comparison; the GPU must have done every unit
@@ -108,3 +109,17 @@ def test_reference_gapsieve_on_the_gpu_matches_its_cpu_build(args, tmp_path):
     assert len(cpu_lines) > 0
     assert gpu_lines == cpu_lines
     assert gpu_counts == cpu_counts
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("env", [{"GAPSIEVE_GPU_CAP": "1000"}, {"GAPSIEVE_GPU_SPLIT": "0", "GAPSIEVE_GPU_UNIT": "3"}])
+def test_reference_host_protocol_paths(env, tmp_path):
+    """The host's own switches (gapchain/gapsieve_cuda_host.c:18-21): lists of 1000 entries
+    overflow on every unit, so the host enlarges them with cu_grow and resubmits; SPLIT 0 sends
+    every member to the tail kernel, in units of three segments."""
+    args = "-l 9 -g both -s 1000000000000000 -e 1000100000000000"
+    cpu_lines, cpu_counts = run("gapsieve_cpu", args)
+    gpu_lines, gpu_counts = run("gapsieve_gpu", args + " -t 0 --gpu", log=tmp_path / "gpu.log", env=env)
+    assert (gpu_lines, gpu_counts) == (cpu_lines, cpu_counts)
+    if "GAPSIEVE_GPU_CAP" in env:
+        assert "enlarged" in open(tmp_path / "gpu.log").read()
