@@ -174,6 +174,15 @@ int mp_gap_chains(mp_handle *h, uint64_t lo, uint64_t hi, uint32_t min_len, uint
 int mp_chain_sieve(mp_handle *h, uint64_t lo, uint64_t hi, uint32_t k, uint32_t shape, uint64_t *heads,
                    uint32_t *lens, size_t cap, size_t *count);
 
+/* the first chain of at least k primes (4 <= k < MP_CHAIN_MAX) whose key lies in [lo, hi), as
+ * gapsieve --first finds it (gapchain/gapsieve.c:1202-1230, the hit ranked by key): the range is
+ * sieved in ascending runs and the call returns after the first run that holds a chain.  The
+ * key is the head for MP_CHAIN_INC and, for MP_CHAIN_DEC, the start of the k-prime pattern that
+ * ends the chain (what A263049 records); *head is the chain's first prime, *len its length
+ * (capped at MP_CHAIN_MAX - 1); *len = 0 when [lo, hi) holds none. */
+int mp_chain_first(mp_handle *h, uint64_t lo, uint64_t hi, uint32_t k, uint32_t shape, uint64_t *key,
+                   uint64_t *head, uint32_t *len);
+
 /* a prime constellation by the same sieve: *count = the number of p in [lo, hi) with p + offs[i]
  * prime for every i (members may lie beyond hi), *cks = the sum of mix64(p) mod 2^64 over them.
  * offs[0] = 0 < offs[1] < ... < offs[k-1] <= MP_TUPLE_MAXOFF, all even, 2 <= k <= MP_TUPLE_MAXK,

@@ -119,6 +119,7 @@ def lib():
             "mp_gap_chains": ([vp, u64, u64, u32, vp, vp, C.c_size_t, C.POINTER(C.c_size_t)], C.c_int),
             "mp_chain_sieve": ([vp, u64, u64, u32, u32, vp, vp, C.c_size_t, C.POINTER(C.c_size_t)], C.c_int),
             "mp_tuple_count": ([vp, u64, u64, vp, u32, C.POINTER(u64), C.POINTER(u64)], C.c_int),
+            "mp_chain_first": ([vp, u64, u64, u32, u32, C.POINTER(u64), C.POINTER(u64), C.POINTER(u32)], C.c_int),
             "mp_autotune": ([vp, u64, C.c_char_p, C.c_size_t], C.c_int),
             "mp_profile_enable": ([vp, C.c_int], C.c_int),
             "mp_profile_read": ([vp, vp, vp, C.c_int], C.c_int),
@@ -287,6 +288,14 @@ class Engine:
         lens = np.zeros(max(1, n.value), dtype=np.uint32)
         self._check(lib().mp_chain_sieve(self._h, lo, hi, k, shape, _p(heads), _p(lens), n.value, C.byref(n)))
         return heads[:n.value], lens[:n.value]
+
+    def chain_first(self, lo, hi, k, dec=False):
+        """The first chain of at least k primes with its key in [lo, hi) (mp_chain_first):
+        (key, first prime, length), or None when there is none."""
+        key, head, n = C.c_uint64(), C.c_uint64(), C.c_uint32()
+        self._check(lib().mp_chain_first(self._h, lo, hi, k, 1 if dec else 0, C.byref(key), C.byref(head),
+                                         C.byref(n)))
+        return (key.value, head.value, n.value) if n.value else None
 
     def tuple_count(self, lo, hi, offs):
         """(count, checksum) of the p in [lo, hi) with p + o prime for every o in offs

@@ -624,8 +624,10 @@ static int cs_prepare(mp_handle *h, u32 mode, const std::vector<u32> &offs)
 // every candidate of [lo, hi): the odd p below CS_SIEVE_LO (where a member may be a sieve
 // prime) as one list, then the sieve's units; collect(list, count on the device, capacity,
 // base, expected survivors) checks each list exactly
-template <class Collect>
-static int cs_sieve_range(mp_handle *h, ChainDev &D, u64 lo, u64 hi, cudaStream_t st, Collect &&collect)
+// done() is asked after the strip and after every run of segments (all its classes): true ends
+// the range there (candidates come in ascending runs, so an earlier run holds smaller p)
+template <class Collect, class Done>
+static int cs_sieve_range(mp_handle *h, ChainDev &D, u64 lo, u64 hi, cudaStream_t st, Collect &&collect, Done &&done)
 {
     const CsPlan &P = D.plan;
     if (lo < CS_SIEVE_LO) {
@@ -638,6 +640,7 @@ static int cs_sieve_range(mp_handle *h, ChainDev &D, u64 lo, u64 hi, cudaStream_
             MP_TRY(collect(D.l0.as<u64>(), D.cnt.as<ull>(), n, (u64)0, n));
         }
     }
+    if (done()) return MP_OK;
     const u64 slo = std::max<u64>(lo, CS_SIEVE_LO);
     if (!D.ok || slo >= hi) return MP_OK;
     const u64 W = P.W, segsize = (u64)CS_K * W;
@@ -680,9 +683,12 @@ static int cs_sieve_range(mp_handle *h, ChainDev &D, u64 lo, u64 hi, cudaStream_
                 break;
             }
         }
+        if (done()) return MP_OK;
     }
     return MP_OK;
 }
+
+static bool cs_never() { return false; }
 
 // verify a survivor list (offsets from base, count on the device) and append the chains
 static int cs_collect(mp_handle *h, ChainDev &D, const u64 *list, const ull *nin, u64 cap, u64 base, u64 expect,
@@ -738,9 +744,12 @@ extern "C" int mp_chain_sieve(mp_handle *h, uint64_t lo, uint64_t hi, uint32_t k
     D.kept = false;
     std::vector<u64> H;
     std::vector<u32> L;
-    MP_TRY(cs_sieve_range(h, D, lo, hi, st, [&](const u64 *list, const ull *nin, u64 cap_, u64 base, u64 expect) {
-        return cs_collect(h, D, list, nin, cap_, base, expect, H, L, st);
-    }));
+    MP_TRY(cs_sieve_range(
+        h, D, lo, hi, st,
+        [&](const u64 *list, const ull *nin, u64 cap_, u64 base, u64 expect) {
+            return cs_collect(h, D, list, nin, cap_, base, expect, H, L, st);
+        },
+        cs_never));
     sort_chains(H, L);
     const size_t m = std::min(cap, H.size());
     std::copy(H.begin(), H.begin() + m, heads);
@@ -752,6 +761,40 @@ extern "C" int mp_chain_sieve(mp_handle *h, uint64_t lo, uint64_t hi, uint32_t k
         D.kept_hi = hi;
         D.kept_h.swap(H);
         D.kept_l.swap(L);
+    }
+    return MP_OK;
+}
+
+extern "C" int mp_chain_first(mp_handle *h, uint64_t lo, uint64_t hi, uint32_t k, uint32_t shape, uint64_t *key,
+                              uint64_t *head, uint32_t *len)
+{
+    if (!h || !key || !head || !len) return MP_EINVAL;
+    *key = *head = 0;
+    *len = 0;
+    if (shape > 1) return mp_set_error(h, MP_EINVAL, "shape must be MP_CHAIN_INC or MP_CHAIN_DEC");
+    if (k < 4 || k > CS_MAXLEN) return mp_set_error(h, MP_EINVAL, "k must be in 4..%d", CS_MAXLEN);
+    if (hi > MP_CHAIN_SIEVE_HI_MAX) return mp_set_error(h, MP_ERANGE, "hi must be <= 2^64 - 2^12");
+    if (hi <= lo) return MP_OK;
+    std::lock_guard<std::recursive_mutex> lk(h->mu);
+    MP_CUDA(h, cudaSetDevice(h->device));
+    cudaStream_t st = h->stream;
+    MP_TRY(cs_prepare(h, shape, chain_offsets(k, shape)));
+    ChainDev &D = *h->chain;
+    D.kept = false;
+    std::vector<u64> H;
+    std::vector<u32> L;
+    MP_TRY(cs_sieve_range(
+        h, D, lo, hi, st,
+        [&](const u64 *list, const ull *nin, u64 cap_, u64 base, u64 expect) {
+            return cs_collect(h, D, list, nin, cap_, base, expect, H, L, st);
+        },
+        [&]() { return !H.empty(); }));
+    // the smallest key: the head for gaps 2, 4, ...; the start of the k-prime pattern that ends
+    // a chain of ..., 4, 2 (member len - k of that chain)
+    for (size_t i = 0; i < H.size(); i++) {
+        const u64 j = L[i] - k;
+        const u64 kk = shape == 0 ? H[i] : H[i] + j * (2 * (u64)L[i] - 1 - j);
+        if (!*len || kk < *key) { *key = kk; *head = H[i]; *len = L[i]; }
     }
     return MP_OK;
 }
@@ -780,7 +823,7 @@ extern "C" int mp_tuple_count(mp_handle *h, uint64_t lo, uint64_t hi, const uint
         const u64 grid = std::max<u64>(1, std::min<u64>((expect + 127) / 128, (u64)h->sm_count * 16));
         cs_tuple_kernel<<<(unsigned)grid, 128, 0, st>>>(list, nin, cap_, base, D.offs.as<u32>(), D.k, acc);
         return cudaGetLastError() == cudaSuccess ? MP_OK : mp_set_error(h, MP_ECUDA, "tuple kernel launch failed");
-    }));
+    }, cs_never));
     ull r[2] = {0, 0};
     MP_CUDA(h, cudaMemcpyAsync(r, acc, sizeof r, cudaMemcpyDeviceToHost, st));
     MP_CUDA(h, cudaStreamSynchronize(st));

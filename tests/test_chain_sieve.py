@@ -148,3 +148,17 @@ def test_both_shapes_match_the_reference_program(engine, lo, hi, k):
         heads, lens = engine.chain_sieve(lo, hi, k, dec=dec)
         got |= {(tag, int(h), int(n)) for h, n in zip(heads, lens)}
     assert len(want) > 0 and got == want
+
+
+# ---- GPU: the first chain (gapsieve --first) ----
+
+@pytest.mark.gpu
+def test_chain_first_finds_the_terms(engine, ref_vectors):
+    a, d = ref_vectors["A016045"], ref_vectors["A263049"]
+    assert engine.chain_first(0, 2 ** 63, 13) == (a[11], a[11], 13)           # A016045 a(12)
+    assert engine.chain_first(0, 2 ** 63, 11, dec=True) == (d[9], d[9], 11)   # A263049 a(10)
+    assert engine.chain_first(0, 2 ** 63, 10, dec=True) == (d[8], d[9], 11)   # a(9): the end of that chain
+    # the records, from 1e16 below them
+    assert engine.chain_first(a[14] - 10 ** 16, 2 ** 63, 16) == (a[14], a[14], 16)
+    assert engine.chain_first(d[13] - 10 ** 16, 2 ** 63, 15, dec=True) == (d[13], d[14], 16)
+    assert engine.chain_first(10 ** 12, 10 ** 12 + 10 ** 9, 20) is None
