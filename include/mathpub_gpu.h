@@ -183,6 +183,19 @@ int mp_chain_sieve(mp_handle *h, uint64_t lo, uint64_t hi, uint32_t k, uint32_t 
 int mp_chain_first(mp_handle *h, uint64_t lo, uint64_t hi, uint32_t k, uint32_t shape, uint64_t *key,
                    uint64_t *head, uint32_t *len);
 
+/* the same two calls for ranges above 2^64, as the reference's gapsieve searches them: lo, hi,
+ * the heads and the keys are 128-bit numbers given as (low word, high word) pairs, and
+ * hi <= 3.3e24 (MP_CHAIN128_HI_MAX_W1 2^64 + MP_CHAIN128_HI_MAX_W0), below which Miller-Rabin
+ * with the 13 prime bases 2..41 proves primality (Sorenson and Webster 2015; the bound of
+ * gapchain/gapsieve.c, PSI13).  Members below 2^64 are certified by BPSW, the others by those
+ * 13 bases; heads[2 i], heads[2 i + 1] hold chain i.  k >= 4 for both shapes. */
+#define MP_CHAIN128_HI_MAX_W1 178893ull
+#define MP_CHAIN128_HI_MAX_W0 6612421877182758912ull
+int mp_chain_sieve128(mp_handle *h, const uint64_t lo[2], const uint64_t hi[2], uint32_t k, uint32_t shape,
+                      uint64_t *heads, uint32_t *lens, size_t cap, size_t *count);
+int mp_chain_first128(mp_handle *h, const uint64_t lo[2], const uint64_t hi[2], uint32_t k, uint32_t shape,
+                      uint64_t key[2], uint64_t head[2], uint32_t *len);
+
 /* a prime constellation by the same sieve: *count = the number of p in [lo, hi) with p + offs[i]
  * prime for every i (members may lie beyond hi), *cks = the sum of mix64(p) mod 2^64 over them.
  * offs[0] = 0 < offs[1] < ... < offs[k-1] <= MP_TUPLE_MAXOFF, all even, 2 <= k <= MP_TUPLE_MAXK,

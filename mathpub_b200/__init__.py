@@ -120,6 +120,8 @@ def lib():
             "mp_chain_sieve": ([vp, u64, u64, u32, u32, vp, vp, C.c_size_t, C.POINTER(C.c_size_t)], C.c_int),
             "mp_tuple_count": ([vp, u64, u64, vp, u32, C.POINTER(u64), C.POINTER(u64)], C.c_int),
             "mp_chain_first": ([vp, u64, u64, u32, u32, C.POINTER(u64), C.POINTER(u64), C.POINTER(u32)], C.c_int),
+            "mp_chain_sieve128": ([vp, vp, vp, u32, u32, vp, vp, C.c_size_t, C.POINTER(C.c_size_t)], C.c_int),
+            "mp_chain_first128": ([vp, vp, vp, u32, u32, vp, vp, C.POINTER(u32)], C.c_int),
             "mp_autotune": ([vp, u64, C.c_char_p, C.c_size_t], C.c_int),
             "mp_profile_enable": ([vp, C.c_int], C.c_int),
             "mp_profile_read": ([vp, vp, vp, C.c_int], C.c_int),
@@ -296,6 +298,34 @@ class Engine:
         self._check(lib().mp_chain_first(self._h, lo, hi, k, 1 if dec else 0, C.byref(key), C.byref(head),
                                          C.byref(n)))
         return (key.value, head.value, n.value) if n.value else None
+
+    @staticmethod
+    def _w2(x):
+        return np.array([x & (2 ** 64 - 1), x >> 64], dtype=np.uint64)
+
+    def chain_sieve128(self, lo, hi, k, dec=False):
+        """chain_sieve for 128-bit ranges (mp_chain_sieve128, hi <= 3.3e24): a list of
+        (first prime, length) with Python integers, ascending."""
+        shape = 1 if dec else 0
+        wl, wh = self._w2(lo), self._w2(hi)
+        n = C.c_size_t()
+        self._check(lib().mp_chain_sieve128(self._h, _p(wl), _p(wh), k, shape, None, None, 0, C.byref(n)))
+        heads = np.zeros(2 * max(1, n.value), dtype=np.uint64)
+        lens = np.zeros(max(1, n.value), dtype=np.uint32)
+        self._check(lib().mp_chain_sieve128(self._h, _p(wl), _p(wh), k, shape, _p(heads), _p(lens), n.value,
+                                            C.byref(n)))
+        return [(int(heads[2 * i]) | int(heads[2 * i + 1]) << 64, int(lens[i])) for i in range(n.value)]
+
+    def chain_first128(self, lo, hi, k, dec=False):
+        """chain_first for 128-bit ranges (mp_chain_first128): (key, first prime, length) or None."""
+        wl, wh = self._w2(lo), self._w2(hi)
+        key, head = np.zeros(2, dtype=np.uint64), np.zeros(2, dtype=np.uint64)
+        n = C.c_uint32()
+        self._check(lib().mp_chain_first128(self._h, _p(wl), _p(wh), k, 1 if dec else 0, _p(key), _p(head),
+                                            C.byref(n)))
+        if not n.value:
+            return None
+        return int(key[0]) | int(key[1]) << 64, int(head[0]) | int(head[1]) << 64, n.value
 
     def tuple_count(self, lo, hi, offs):
         """(count, checksum) of the p in [lo, hi) with p + o prime for every o in offs

@@ -136,6 +136,61 @@ __device__ bool is_prime_exact(u64 x)
     return bpsw_odd(x);
 }
 
+// the strong probable-prime test to base a (2 <= a < n) for odd n >= 2^64 below 2^127, with
+// one = R mod n and r2 = R^2 mod n (R = 2^128), n - 1 = d 2^s
+__device__ bool mr_w2(w2 n, u64 ni, w2 one, w2 r2, w2 d, int s, u32 a)
+{
+    const w2 am = w2_mmul(w2{a, 0}, r2, n, ni);         // a R mod n
+    const w2 mone = w2_sub(n, one);
+    w2 x = am;                                          // for the top bit of d
+    const int top = d.hi ? 127 - __clzll((long long)d.hi) : 63 - __clzll((long long)d.lo);
+    for (int i = top - 1; i >= 0; i--) {
+        x = w2_mmul(x, x, n, ni);
+        const u64 bit = i >= 64 ? (d.hi >> (i - 64)) & 1 : (d.lo >> i) & 1;
+        if (bit) x = w2_mmul(x, am, n, ni);
+    }
+    if (w2_eq(x, one) || w2_eq(x, mone)) return true;
+    for (int i = 1; i < s; i++) {
+        x = w2_mmul(x, x, n, ni);
+        if (w2_eq(x, mone)) return true;
+        if (w2_eq(x, one)) return false;
+    }
+    return false;
+}
+
+// exact primality below 3.317e24: BPSW below 2^64; above, Miller-Rabin with the 13 prime bases
+// 2..41, which no composite below 3,317,044,064,679,887,385,961,981 passes (Sorenson and
+// Webster, 2015), after trial division by the primes to 41
+__device__ bool is_prime_w2(w2 n)
+{
+    if (!n.hi) return is_prime_exact(n.lo);
+    if (!(n.lo & 1)) return false;
+    const u32 B[13] = {2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37, 41};
+    // n mod q from the two words: (hi 2^64 + lo) mod q, 2^64 mod q by (2^64 - 1) mod q + 1
+    for (int i = 1; i < 13; i++) {
+        const u64 q = B[i], t = (~0ull % q + 1) % q;
+        if (((n.hi % q) * t + n.lo % q) % q == 0) return false;
+    }
+    const u64 ni = 0 - m_inv(n.lo);
+    const int b = 127 - __clzll((long long)n.hi);
+    w2 one = w2{0, 1ull << (b - 64)};
+    for (int i = b; i < 128; i++) one = w2_madd(one, one, n);
+    w2 r2 = one;
+    for (int i = 0; i < 128; i++) r2 = w2_madd(r2, r2, n);
+    w2 d = w2_sub(n, w2{1, 0});
+    int s = 0;
+    if (!d.lo) { s = 64; d.lo = d.hi; d.hi = 0; }
+    const int z = __ffsll((long long)d.lo) - 1;
+    if (z) { d.lo = (d.lo >> z) | (d.hi << (64 - z)); d.hi >>= z; }
+    s += z;
+    for (int i = 0; i < 13; i++)
+        if (!mr_w2(n, ni, one, r2, d, s, B[i])) return false;
+    return true;
+}
+
+__device__ __forceinline__ w2 w2_addu(w2 a, u64 b) { const u64 lo = a.lo + b; return w2{lo, a.hi + (lo < b)}; }
+__device__ __forceinline__ w2 w2_subu(w2 a, u64 b) { return w2{a.lo - b, a.hi - (a.lo < b)}; }
+
 // ---- the kernels ----
 
 struct CsTables {                             // shared by both shapes and every unit
@@ -317,25 +372,26 @@ __global__ void __launch_bounds__(256) cs_screen_tail(const u64 *__restrict__ in
     }
 }
 
-// mp_chain_sieve's exact check of the screen's survivors p = base + off (all below 2^64):
-// shape 0 (gaps 2, 4, ...): members p + m(m + 1) prime and the odd numbers between them
-// composite, extended forwards; shape 1 (..., 4, 2): the k-member pattern p + m(2k - 1 - m)
-// exact, then extended backwards while the gap before the first prime is 2 len.  Chains of
-// CS_MAXLEN primes are not extended further.
-__global__ void __launch_bounds__(128) cs_verify_kernel(const u64 *__restrict__ in, const ull *nin, u64 cap, u64 base,
-                                                        u32 k, u32 shape, u64 *heads, u32 *lens, ull *nres)
+// mp_chain_sieve's exact check of the screen's survivors p = base + off (128-bit): shape 0
+// (gaps 2, 4, ...): members p + m(m + 1) prime and the odd numbers between them composite,
+// extended forwards; shape 1 (..., 4, 2): the k-member pattern p + m(2k - 1 - m) exact, then
+// extended backwards while the gap before the first prime is 2 len.  Chains of CS_MAXLEN primes
+// are not extended further.  Heads are written as (low, high) word pairs.
+__global__ void __launch_bounds__(128) cs_verify_kernel(const u64 *__restrict__ in, const ull *nin, u64 cap,
+                                                        u64 base_lo, u64 base_hi, u32 k, u32 shape, u64 *heads,
+                                                        u32 *lens, ull *nres)
 {
     const u64 n = min((u64)*nin, cap);
     for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
-        const u64 p = base + in[i];
-        u64 head = p;
+        const w2 p = w2_addu(w2{base_lo, base_hi}, in[i]);
+        w2 head = p;
         u32 len = 0;
         if (shape == 0) {
             for (u32 m = 0; m < CS_MAXLEN; m++) {
-                const u64 x = p + (u64)m * (m + 1);
-                if (!is_prime_exact(x)) break;
+                const w2 x = w2_addu(p, (u64)m * (m + 1));
+                if (!is_prime_w2(x)) break;
                 bool clear = true;
-                for (u64 y = x - 2 * (u64)m + 2; m && y < x && clear; y += 2) clear = !is_prime_exact(y);
+                for (u32 t = 1; m && t < m && clear; t++) clear = !is_prime_w2(w2_subu(x, 2 * (u64)t));
                 if (!clear) break;
                 len = m + 1;
             }
@@ -343,18 +399,18 @@ __global__ void __launch_bounds__(128) cs_verify_kernel(const u64 *__restrict__ 
         } else {
             bool ok = true;
             for (u32 m = 0; m < k && ok; m++) {
-                const u64 x = p + (u64)m * (2 * k - 1 - m);
-                ok = is_prime_exact(x);
-                for (u64 y = x + 2; ok && m + 1 < k && y < x + 2 * (u64)(k - 1 - m); y += 2) ok = !is_prime_exact(y);
+                const w2 x = w2_addu(p, (u64)m * (2 * k - 1 - m));
+                ok = is_prime_w2(x);
+                for (u32 t = 1; ok && m + 1 < k && t < k - 1 - m; t++) ok = !is_prime_w2(w2_addu(x, 2 * (u64)t));
             }
             if (ok) {
                 len = k;
                 while (len < CS_MAXLEN) {
                     const u64 gap = 2 * (u64)len;
-                    if (head < gap + 3) break;
-                    const u64 prev = head - gap;
-                    bool step = is_prime_exact(prev);
-                    for (u64 y = prev + 2; step && y < head; y += 2) step = !is_prime_exact(y);
+                    if (!head.hi && head.lo < gap + 3) break;
+                    const w2 prev = w2_subu(head, gap);
+                    bool step = is_prime_w2(prev);
+                    for (u32 t = 1; step && t < len; t++) step = !is_prime_w2(w2_addu(prev, 2 * (u64)t));
                     if (!step) break;
                     head = prev;
                     len++;
@@ -363,7 +419,7 @@ __global__ void __launch_bounds__(128) cs_verify_kernel(const u64 *__restrict__ 
         }
         if (len) {
             const ull j = atomicAdd(nres, 1ull);
-            if (j < cap) { heads[j] = head; lens[j] = len; }
+            if (j < cap) { heads[2 * j] = head.lo; heads[2 * j + 1] = head.hi; lens[j] = len; }
         }
     }
 }
@@ -513,21 +569,21 @@ bool make_plan(const std::vector<u32> &offs, CsPlan &P)
     return true;
 }
 
-// LSD radix sort of (head, len) pairs by head, skipping the digits where all heads agree
-void sort_chains(std::vector<u64> &H, std::vector<u32> &L)
+// LSD radix sort of (head, len) pairs by head (128-bit), skipping the digits where all heads agree
+void sort_chains(std::vector<u128t> &H, std::vector<u32> &L)
 {
     const size_t n = H.size();
     if (n < 2) return;
-    std::vector<u64> h2(n);
+    std::vector<u128t> h2(n);
     std::vector<u32> l2(n);
-    for (int sh = 0; sh < 64; sh += 11) {
+    for (int sh = 0; sh < 128; sh += 11) {
         std::vector<size_t> cnt(2048, 0);
-        for (u64 v : H) cnt[(v >> sh) & 2047]++;
+        for (const u128t &v : H) cnt[(size_t)(v >> sh) & 2047]++;
         if (*std::max_element(cnt.begin(), cnt.end()) == n) continue;
         size_t pos = 0;
         for (size_t &c : cnt) { const size_t t = c; c = pos; pos += t; }
         for (size_t i = 0; i < n; i++) {
-            const size_t d = cnt[(H[i] >> sh) & 2047]++;
+            const size_t d = cnt[(size_t)(H[i] >> sh) & 2047]++;
             h2[d] = H[i];
             l2[d] = L[i];
         }
@@ -562,7 +618,7 @@ __global__ void __launch_bounds__(128) cs_tuple_kernel(const u64 *__restrict__ i
     }
 }
 
-// ---- mp_chain_sieve and mp_tuple_count: one plan and one set of buffers per handle ----
+// ---- mp_chain_sieve, mp_chain_first and mp_tuple_count: one plan and buffers per handle ----
 
 #define CS_MODE_TUPLE 2u                       // modes 0 and 1 are the chain shapes
 
@@ -574,8 +630,8 @@ struct ChainDev {
     // the last chain list when the caller's arrays were too small, for the call that follows
     // with room for all of it (count first, then fill) so that the range is not sieved twice
     bool kept = false;
-    u64 kept_lo = 0, kept_hi = 0;
-    std::vector<u64> kept_h;
+    u128t kept_lo = 0, kept_hi = 0;
+    std::vector<u128t> kept_h;
     std::vector<u32> kept_l;
     DevBuf ginfo, q, qinv, crt, pat, res, offs, bq, l0, l1, cnt, rh, rl;
     void release()
@@ -621,31 +677,33 @@ static int cs_prepare(mp_handle *h, u32 mode, const std::vector<u32> &offs)
     return MP_OK;
 }
 
-// every candidate of [lo, hi): the odd p below CS_SIEVE_LO (where a member may be a sieve
-// prime) as one list, then the sieve's units; collect(list, count on the device, capacity,
-// base, expected survivors) checks each list exactly
-// done() is asked after the strip and after every run of segments (all its classes): true ends
-// the range there (candidates come in ascending runs, so an earlier run holds smaller p)
+// every candidate of [lo, hi) (128-bit): the odd p below CS_SIEVE_LO (where a member may be a
+// sieve prime) as one list, then the sieve's units.  collect(list, count on the device,
+// capacity, base, expected survivors) checks each list exactly; done() is asked after the
+// strip and after every run of segments (all its classes): true ends the range there
+// (candidates come in ascending runs, so an earlier run holds smaller p).
 template <class Collect, class Done>
-static int cs_sieve_range(mp_handle *h, ChainDev &D, u64 lo, u64 hi, cudaStream_t st, Collect &&collect, Done &&done)
+static int cs_sieve_range(mp_handle *h, ChainDev &D, u128t lo, u128t hi, cudaStream_t st, Collect &&collect,
+                          Done &&done)
 {
     const CsPlan &P = D.plan;
     if (lo < CS_SIEVE_LO) {
         std::vector<u64> strip;
-        for (u64 p = std::max<u64>(lo, 3) | 1; p < std::min<u64>(hi, CS_SIEVE_LO); p += 2) strip.push_back(p);
+        const u64 e = hi < CS_SIEVE_LO ? (u64)hi : CS_SIEVE_LO;
+        for (u64 p = std::max<u64>((u64)lo, 3) | 1; p < e; p += 2) strip.push_back(p);
         if (!strip.empty()) {
             MP_CUDA(h, upload(D.l0, strip));
             const ull n = strip.size();
             MP_CUDA(h, cudaMemcpy(D.cnt.p, &n, sizeof n, cudaMemcpyHostToDevice));
-            MP_TRY(collect(D.l0.as<u64>(), D.cnt.as<ull>(), n, (u64)0, n));
+            MP_TRY(collect(D.l0.as<u64>(), D.cnt.as<ull>(), n, (u128t)0, n));
         }
     }
     if (done()) return MP_OK;
-    const u64 slo = std::max<u64>(lo, CS_SIEVE_LO);
+    const u128t slo = lo > CS_SIEVE_LO ? lo : (u128t)CS_SIEVE_LO;
     if (!D.ok || slo >= hi) return MP_OK;
     const u64 W = P.W, segsize = (u64)CS_K * W;
     const u32 A = (u32)P.res.size(), nps = (u32)P.q.size();
-    const u64 nseg_all = (hi - slo + segsize - 1) / segsize;
+    const u64 nseg_all = (u64)((hi - slo + segsize - 1) / segsize);
     // units: runs of segments (or, for dense patterns, runs of classes of one segment) sized
     // for about 2^24 expected sieve survivors
     const double per_class = (double)CS_K * P.survive, target = 16777216.0;
@@ -660,13 +718,15 @@ static int cs_sieve_range(mp_handle *h, ChainDev &D, u64 lo, u64 hi, cudaStream_
     MP_CUDA(h, D.bq.ensure(bq.size() * 4));
     for (u64 s = 0; s < nseg_all; s += useg) {
         const u32 ns = (u32)std::min<u64>(useg, nseg_all - s);
-        const u64 base = slo + s * segsize;
+        const u128t base = slo + (u128t)s * segsize;
         for (u32 g = 0; g < ns; g++)
-            for (u32 i = 0; i < nps; i++) bq[(size_t)g * nps + i] = (u32)((base + g * segsize) % P.q[i]);
+            for (u32 i = 0; i < nps; i++) bq[(size_t)g * nps + i] = (u32)((base + (u128t)g * segsize) % P.q[i]);
         MP_CUDA(h, cudaMemcpyAsync(D.bq.p, bq.data(), (size_t)ns * nps * 4, cudaMemcpyHostToDevice, st));
+        const u128t room = hi - 1 - base;
+        const u64 lim = room > (u128t)~0ull ? ~0ull : (u64)room;
         for (u32 j0 = 0; j0 < A; j0 += ucls) {
-            const CsUnit U{base, 0, hi - 1 - base, segsize, (u32)W, (u32)(base % W), ns, j0, std::min(ucls, A - j0),
-                           D.bq.as<u32>()};
+            const CsUnit U{(u64)base, (u64)(base >> 64), lim, segsize, (u32)W, (u32)(base % W), ns, j0,
+                           std::min(ucls, A - j0), D.bq.as<u32>()};
             for (;;) {
                 MP_CUDA(h, D.l0.ensure(ucap * 8));
                 MP_CUDA(h, D.l1.ensure(ucap * 8));
@@ -691,30 +751,70 @@ static int cs_sieve_range(mp_handle *h, ChainDev &D, u64 lo, u64 hi, cudaStream_
 static bool cs_never() { return false; }
 
 // verify a survivor list (offsets from base, count on the device) and append the chains
-static int cs_collect(mp_handle *h, ChainDev &D, const u64 *list, const ull *nin, u64 cap, u64 base, u64 expect,
-                      std::vector<u64> &H, std::vector<u32> &L, cudaStream_t st)
+static int cs_collect(mp_handle *h, ChainDev &D, const u64 *list, const ull *nin, u64 cap, u128t base, u64 expect,
+                      std::vector<u128t> &H, std::vector<u32> &L, cudaStream_t st)
 {
     ull *nres = D.cnt.as<ull>() + CS_CNT_RES;
-    MP_CUDA(h, D.rh.ensure(cap * 8));
+    MP_CUDA(h, D.rh.ensure(cap * 16));
     MP_CUDA(h, D.rl.ensure(cap * 4));
     MP_CUDA(h, cudaMemsetAsync(nres, 0, sizeof(ull), st));
     const u64 grid = std::max<u64>(1, std::min<u64>((expect + 127) / 128, (u64)h->sm_count * 16));
-    cs_verify_kernel<<<(unsigned)grid, 128, 0, st>>>(list, nin, cap, base, D.k, D.mode, D.rh.as<u64>(), D.rl.as<u32>(),
-                                                     nres);
+    cs_verify_kernel<<<(unsigned)grid, 128, 0, st>>>(list, nin, cap, (u64)base, (u64)(base >> 64), D.k, D.mode,
+                                                     D.rh.as<u64>(), D.rl.as<u32>(), nres);
     MP_CUDA(h, cudaGetLastError());
     ull nr = 0;
     MP_CUDA(h, cudaMemcpyAsync(&nr, nres, sizeof nr, cudaMemcpyDeviceToHost, st));
     MP_CUDA(h, cudaStreamSynchronize(st));
     if (nr > cap) return mp_set_error(h, MP_EOVERFLOW, "chain sieve: more chains than survivors");
     if (nr) {
+        std::vector<u64> w(2 * nr);
         const size_t o = H.size();
-        H.resize(o + nr);
         L.resize(o + nr);
-        MP_CUDA(h, cudaMemcpyAsync(H.data() + o, D.rh.p, nr * 8, cudaMemcpyDeviceToHost, st));
+        MP_CUDA(h, cudaMemcpyAsync(w.data(), D.rh.p, nr * 16, cudaMemcpyDeviceToHost, st));
         MP_CUDA(h, cudaMemcpyAsync(L.data() + o, D.rl.p, nr * 4, cudaMemcpyDeviceToHost, st));
         MP_CUDA(h, cudaStreamSynchronize(st));
+        H.resize(o + nr);
+        for (size_t i = 0; i < nr; i++) H[o + i] = (u128t)w[2 * i + 1] << 64 | w[2 * i];
     }
     return MP_OK;
+}
+
+static const u128t CS_HI128_MAX = (u128t)MP_CHAIN128_HI_MAX_W1 << 64 | MP_CHAIN128_HI_MAX_W0;
+
+// the chains with keys in [lo, hi), sorted by head; *H and *L receive them (the kept list when
+// the previous call asked for the same range with too little room)
+static int cs_chains(mp_handle *h, u128t lo, u128t hi, u32 k, u32 shape, std::vector<u128t> &H, std::vector<u32> &L)
+{
+    cudaStream_t st = h->stream;
+    MP_TRY(cs_prepare(h, shape, chain_offsets(k, shape)));
+    ChainDev &D = *h->chain;
+    if (D.kept && D.kept_lo == lo && D.kept_hi == hi) {
+        H.swap(D.kept_h);
+        L.swap(D.kept_l);
+        D.kept = false;
+        return MP_OK;
+    }
+    D.kept = false;
+    MP_TRY(cs_sieve_range(
+        h, D, lo, hi, st,
+        [&](const u64 *list, const ull *nin, u64 cap_, u128t base, u64 expect) {
+            return cs_collect(h, D, list, nin, cap_, base, expect, H, L, st);
+        },
+        cs_never));
+    sort_chains(H, L);
+    return MP_OK;
+}
+
+// keep what did not fit for the next call with the same range
+static void cs_keep(mp_handle *h, u128t lo, u128t hi, size_t cap, std::vector<u128t> &H, std::vector<u32> &L)
+{
+    if (cap >= H.size()) return;
+    ChainDev &D = *h->chain;
+    D.kept = true;
+    D.kept_lo = lo;
+    D.kept_hi = hi;
+    D.kept_h.swap(H);
+    D.kept_l.swap(L);
 }
 
 extern "C" int mp_chain_sieve(mp_handle *h, uint64_t lo, uint64_t hi, uint32_t k, uint32_t shape, uint64_t *heads,
@@ -730,37 +830,59 @@ extern "C" int mp_chain_sieve(mp_handle *h, uint64_t lo, uint64_t hi, uint32_t k
     if (shape == 0 && k < 4) return mp_gap_chains(h, lo, hi, k, heads, lens, cap, count);   // dense: enumerate
     std::lock_guard<std::recursive_mutex> lk(h->mu);
     MP_CUDA(h, cudaSetDevice(h->device));
+    std::vector<u128t> H;
+    std::vector<u32> L;
+    MP_TRY(cs_chains(h, lo, hi, k, shape, H, L));
+    const size_t m = std::min(cap, H.size());
+    for (size_t i = 0; i < m; i++) { heads[i] = (u64)H[i]; lens[i] = L[i]; }
+    *count = H.size();
+    cs_keep(h, lo, hi, cap, H, L);
+    return MP_OK;
+}
+
+extern "C" int mp_chain_sieve128(mp_handle *h, const uint64_t lo[2], const uint64_t hi[2], uint32_t k, uint32_t shape,
+                                 uint64_t *heads, uint32_t *lens, size_t cap, size_t *count)
+{
+    if (!h || !lo || !hi || !count || (cap && (!heads || !lens))) return MP_EINVAL;
+    *count = 0;
+    if (shape > 1) return mp_set_error(h, MP_EINVAL, "shape must be MP_CHAIN_INC or MP_CHAIN_DEC");
+    if (k < 4 || k > CS_MAXLEN) return mp_set_error(h, MP_EINVAL, "k must be in 4..%d", CS_MAXLEN);
+    const u128t L0 = (u128t)lo[1] << 64 | lo[0], H0 = (u128t)hi[1] << 64 | hi[0];
+    if (H0 > CS_HI128_MAX) return mp_set_error(h, MP_ERANGE, "hi must be <= 3.3e24");
+    if (H0 <= L0) return MP_OK;
+    std::lock_guard<std::recursive_mutex> lk(h->mu);
+    MP_CUDA(h, cudaSetDevice(h->device));
+    std::vector<u128t> H;
+    std::vector<u32> L;
+    MP_TRY(cs_chains(h, L0, H0, k, shape, H, L));
+    const size_t m = std::min(cap, H.size());
+    for (size_t i = 0; i < m; i++) { heads[2 * i] = (u64)H[i]; heads[2 * i + 1] = (u64)(H[i] >> 64); lens[i] = L[i]; }
+    *count = H.size();
+    cs_keep(h, L0, H0, cap, H, L);
+    return MP_OK;
+}
+
+// the first chain: runs in ascending order, stopping after the first run that holds one; the
+// smallest key wins (the head for gaps 2, 4, ...; for ..., 4, 2 the start of the k-prime
+// pattern that ends the chain, member len - k of it)
+static int cs_first(mp_handle *h, u128t lo, u128t hi, u32 k, u32 shape, u128t *key, u128t *head, u32 *len)
+{
     cudaStream_t st = h->stream;
     MP_TRY(cs_prepare(h, shape, chain_offsets(k, shape)));
     ChainDev &D = *h->chain;
-    if (D.kept && D.kept_lo == lo && D.kept_hi == hi) {
-        const size_t m = std::min(cap, D.kept_h.size());
-        std::copy(D.kept_h.begin(), D.kept_h.begin() + m, heads);
-        std::copy(D.kept_l.begin(), D.kept_l.begin() + m, lens);
-        *count = D.kept_h.size();
-        if (m == D.kept_h.size()) { D.kept = false; D.kept_h = {}; D.kept_l = {}; }
-        return MP_OK;
-    }
     D.kept = false;
-    std::vector<u64> H;
+    std::vector<u128t> H;
     std::vector<u32> L;
     MP_TRY(cs_sieve_range(
         h, D, lo, hi, st,
-        [&](const u64 *list, const ull *nin, u64 cap_, u64 base, u64 expect) {
+        [&](const u64 *list, const ull *nin, u64 cap_, u128t base, u64 expect) {
             return cs_collect(h, D, list, nin, cap_, base, expect, H, L, st);
         },
-        cs_never));
-    sort_chains(H, L);
-    const size_t m = std::min(cap, H.size());
-    std::copy(H.begin(), H.begin() + m, heads);
-    std::copy(L.begin(), L.begin() + m, lens);
-    *count = H.size();
-    if (m < H.size()) {
-        D.kept = true;
-        D.kept_lo = lo;
-        D.kept_hi = hi;
-        D.kept_h.swap(H);
-        D.kept_l.swap(L);
+        [&]() { return !H.empty(); }));
+    for (size_t i = 0; i < H.size(); i++) {
+        const u64 j = L[i] - k;
+        const u128t kk = shape == 0 ? H[i] : H[i] + (u128t)(j * (2 * (u64)L[i] - 1 - j));
+        if (!*len || kk < *key) { *key = kk; *head = H[i]; *len = L[i]; }
     }
     return MP_OK;
 }
@@ -777,25 +899,30 @@ extern "C" int mp_chain_first(mp_handle *h, uint64_t lo, uint64_t hi, uint32_t k
     if (hi <= lo) return MP_OK;
     std::lock_guard<std::recursive_mutex> lk(h->mu);
     MP_CUDA(h, cudaSetDevice(h->device));
-    cudaStream_t st = h->stream;
-    MP_TRY(cs_prepare(h, shape, chain_offsets(k, shape)));
-    ChainDev &D = *h->chain;
-    D.kept = false;
-    std::vector<u64> H;
-    std::vector<u32> L;
-    MP_TRY(cs_sieve_range(
-        h, D, lo, hi, st,
-        [&](const u64 *list, const ull *nin, u64 cap_, u64 base, u64 expect) {
-            return cs_collect(h, D, list, nin, cap_, base, expect, H, L, st);
-        },
-        [&]() { return !H.empty(); }));
-    // the smallest key: the head for gaps 2, 4, ...; the start of the k-prime pattern that ends
-    // a chain of ..., 4, 2 (member len - k of that chain)
-    for (size_t i = 0; i < H.size(); i++) {
-        const u64 j = L[i] - k;
-        const u64 kk = shape == 0 ? H[i] : H[i] + j * (2 * (u64)L[i] - 1 - j);
-        if (!*len || kk < *key) { *key = kk; *head = H[i]; *len = L[i]; }
-    }
+    u128t K = 0, Hd = 0;
+    MP_TRY(cs_first(h, lo, hi, k, shape, &K, &Hd, len));
+    *key = (u64)K;
+    *head = (u64)Hd;
+    return MP_OK;
+}
+
+extern "C" int mp_chain_first128(mp_handle *h, const uint64_t lo[2], const uint64_t hi[2], uint32_t k, uint32_t shape,
+                                 uint64_t key[2], uint64_t head[2], uint32_t *len)
+{
+    if (!h || !lo || !hi || !key || !head || !len) return MP_EINVAL;
+    key[0] = key[1] = head[0] = head[1] = 0;
+    *len = 0;
+    if (shape > 1) return mp_set_error(h, MP_EINVAL, "shape must be MP_CHAIN_INC or MP_CHAIN_DEC");
+    if (k < 4 || k > CS_MAXLEN) return mp_set_error(h, MP_EINVAL, "k must be in 4..%d", CS_MAXLEN);
+    const u128t L0 = (u128t)lo[1] << 64 | lo[0], H0 = (u128t)hi[1] << 64 | hi[0];
+    if (H0 > CS_HI128_MAX) return mp_set_error(h, MP_ERANGE, "hi must be <= 3.3e24");
+    if (H0 <= L0) return MP_OK;
+    std::lock_guard<std::recursive_mutex> lk(h->mu);
+    MP_CUDA(h, cudaSetDevice(h->device));
+    u128t K = 0, Hd = 0;
+    MP_TRY(cs_first(h, L0, H0, k, shape, &K, &Hd, len));
+    key[0] = (u64)K; key[1] = (u64)(K >> 64);
+    head[0] = (u64)Hd; head[1] = (u64)(Hd >> 64);
     return MP_OK;
 }
 
@@ -819,11 +946,14 @@ extern "C" int mp_tuple_count(mp_handle *h, uint64_t lo, uint64_t hi, const uint
     ChainDev &D = *h->chain;
     ull *acc = D.cnt.as<ull>() + CS_CNT_TUPLE;
     MP_CUDA(h, cudaMemsetAsync(acc, 0, 2 * sizeof(ull), st));
-    MP_TRY(cs_sieve_range(h, D, lo, hi, st, [&](const u64 *list, const ull *nin, u64 cap_, u64 base, u64 expect) {
-        const u64 grid = std::max<u64>(1, std::min<u64>((expect + 127) / 128, (u64)h->sm_count * 16));
-        cs_tuple_kernel<<<(unsigned)grid, 128, 0, st>>>(list, nin, cap_, base, D.offs.as<u32>(), D.k, acc);
-        return cudaGetLastError() == cudaSuccess ? MP_OK : mp_set_error(h, MP_ECUDA, "tuple kernel launch failed");
-    }, cs_never));
+    MP_TRY(cs_sieve_range(
+        h, D, lo, hi, st,
+        [&](const u64 *list, const ull *nin, u64 cap_, u128t base, u64 expect) {
+            const u64 grid = std::max<u64>(1, std::min<u64>((expect + 127) / 128, (u64)h->sm_count * 16));
+            cs_tuple_kernel<<<(unsigned)grid, 128, 0, st>>>(list, nin, cap_, (u64)base, D.offs.as<u32>(), D.k, acc);
+            return cudaGetLastError() == cudaSuccess ? MP_OK : mp_set_error(h, MP_ECUDA, "tuple kernel launch failed");
+        },
+        cs_never));
     ull r[2] = {0, 0};
     MP_CUDA(h, cudaMemcpyAsync(r, acc, sizeof r, cudaMemcpyDeviceToHost, st));
     MP_CUDA(h, cudaStreamSynchronize(st));

@@ -162,3 +162,37 @@ def test_chain_first_finds_the_terms(engine, ref_vectors):
     assert engine.chain_first(a[14] - 10 ** 16, 2 ** 63, 16) == (a[14], a[14], 16)
     assert engine.chain_first(d[13] - 10 ** 16, 2 ** 63, 15, dec=True) == (d[13], d[14], 16)
     assert engine.chain_first(10 ** 12, 10 ** 12 + 10 ** 9, 20) is None
+
+
+# ---- GPU: above 2^64, to the reference's ceiling ----
+
+@pytest.mark.gpu
+def test_chain_first128_finds_the_records_above_2_64(engine, ref_vectors):
+    """A016045 a(16) = 254345176718302423991 (17 primes) and a(17) = 307223174679659356577 (18
+    primes), A263049 a(16) = 134491669675212201371 (17 primes): the reference's newest terms."""
+    a, d = ref_vectors["A016045"], ref_vectors["A263049"]
+    top = 33 * 10 ** 23
+    for term, k, dec in [(a[15], 17, False), (a[16], 18, False), (d[15], 17, True)]:
+        t0 = time.perf_counter()
+        r = engine.chain_first128(term - 10 ** 16, top, k, dec=dec)
+        print(f"k={k} dec={dec}: {r} in {time.perf_counter() - t0:.2f} s")
+        assert r == (term, term, k)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("lo,hi,k", [(2 ** 64 - 5 * 10 ** 12, 2 ** 64 + 5 * 10 ** 12, 10),
+                                     (10 ** 20, 10 ** 20 + 10 ** 13, 10)])
+def test_chain_sieve128_matches_the_reference_program(engine, lo, hi, k):
+    want = reference_chains(f"-l {k} -g both -s {lo} -e {hi - 1}")
+    got = set()
+    for tag, dec in (("inc", False), ("dec", True)):
+        got |= {(tag, h, n) for h, n in engine.chain_sieve128(lo, hi, k, dec=dec)}
+    assert len(want) > 0 and got == want
+
+
+@pytest.mark.gpu
+def test_chain_sieve128_equals_the_64_bit_call(engine):
+    lo, hi = 10 ** 15, 10 ** 15 + 2 * 10 ** 12
+    for dec in (False, True):
+        h, n = engine.chain_sieve(lo, hi, 8, dec=dec)
+        assert engine.chain_sieve128(lo, hi, 8, dec=dec) == [(int(x), int(y)) for x, y in zip(h, n)]
