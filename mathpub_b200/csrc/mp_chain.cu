@@ -14,17 +14,20 @@
 //   screen    every member of every survivor by the base-2 strong test (a composite verdict
 //             is a proof): one member at a time over the whole list with compaction between
 //             rounds, then the remaining members per candidate
-//   verify    members prime (exact), the odd numbers between them composite, the chain
-//             extended (forwards for gaps 2, 4, ...; backwards for ..., 4, 2, whose pattern
-//             ends every chain it is part of)
+//   verify    members prime (exact: BPSW below 2^64, Miller-Rabin with the 13 prime bases 2..41
+//             above, to 3.3e24), the odd numbers between them composite, the chain extended
+//             (forwards for gaps 2, 4, ...; backwards for ..., 4, 2, whose pattern ends every
+//             chain it is part of)
 //
-// Two front ends share the kernels:
-//   cu_*            the C ABI of gapchain/gapsieve_cuda.h (include/gapsieve_cuda.h), so the
-//                   reference's host program gapchain/gapsieve_cuda_host.c runs unmodified on
-//                   these kernels; its host builds the tables and proves the survivors, up to
-//                   its ceiling 3.3e24 (two-word Montgomery arithmetic above 2^64)
-//   mp_chain_sieve  this library's call: the same tables built here, verification on the GPU
-//                   with BPSW, the chains returned in order like mp_gap_chains
+// Front ends sharing the kernels:
+//   cu_*              the C ABI of gapchain/gapsieve_cuda.h (include/gapsieve_cuda.h), so the
+//                     reference's host program gapchain/gapsieve_cuda_host.c runs unmodified
+//                     on these kernels; its host builds the tables and proves the survivors,
+//                     up to its ceiling 3.3e24 (two-word Montgomery arithmetic above 2^64)
+//   mp_chain_sieve    every chain with its key in a range, in order, like mp_gap_chains; the
+//                     tables built here and the verification on the GPU (and its 128-bit form)
+//   mp_chain_first    the first chain of a range, as gapsieve --first (and its 128-bit form)
+//   mp_tuple_count    count and checksum of a prime constellation (A350826's sextuplets)
 #include "mp_mont64.cuh"
 #include <algorithm>
 #include <numeric>
