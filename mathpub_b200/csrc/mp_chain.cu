@@ -238,7 +238,7 @@ __device__ __forceinline__ void cs_and_group(u32 (&acc)[4][4], const uint4 *__re
 // one CTA per CS_CPB classes of one segment: AND the rotated patterns over each class's 2^17
 // values of k and append the survivors' offsets from the unit's base.  The rotations of all
 // the CTA's classes and groups are taken in parallel before one barrier.
-#define CS_CPB 4u                             // classes per CTA
+#define CS_CPB 8u                             // classes per CTA
 #define CS_CPT (CS_K / 128 / CS_THREADS)      // 128-bit chunks per thread and class
 static_assert(CS_CPT == 4, "cs_and_group takes 4 chunks per thread");
 __global__ void __launch_bounds__(CS_THREADS) cs_sieve_kernel(CsTables T, CsShape S, CsUnit U, u64 *list, u64 cap,
