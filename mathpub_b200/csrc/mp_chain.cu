@@ -37,7 +37,7 @@
 #define CS_THREADS 256u
 #define CS_MAXG 64                            // pattern groups
 #define CS_SIEVE_LO 1024u                     // mp_chain_sieve: heads below this are checked one by one
-#define CS_PMAX 199u                          // mp_chain_sieve: pattern primes up to this
+#define CS_PMAX_LIMIT 509u                    // pattern primes stay below CS_SIEVE_LO
 #define CS_PERIOD_MAX (1u << 24)
 #define CS_MAXLEN (MP_CHAIN_MAX - 1)
 #define CS_NCNT (CU_MAXK + 2)                 // counters per shape: raw, after each round, final
@@ -427,6 +427,54 @@ __global__ void __launch_bounds__(128) cs_verify_kernel(const u64 *__restrict__ 
     }
 }
 
+// the same check when every value of the unit lies below 2^64 - 2^12: one-word arithmetic (and
+// half the registers of the two-word form), heads written as (head, 0) pairs
+__global__ void __launch_bounds__(128) cs_verify64_kernel(const u64 *__restrict__ in, const ull *nin, u64 cap, u64 base,
+                                                          u32 k, u32 shape, u64 *heads, u32 *lens, ull *nres)
+{
+    const u64 n = min((u64)*nin, cap);
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
+        const u64 p = base + in[i];
+        u64 head = p;
+        u32 len = 0;
+        if (shape == 0) {
+            for (u32 m = 0; m < CS_MAXLEN; m++) {
+                const u64 x = p + (u64)m * (m + 1);
+                if (!is_prime_exact(x)) break;
+                bool clear = true;
+                for (u64 y = x - 2 * (u64)m + 2; m && y < x && clear; y += 2) clear = !is_prime_exact(y);
+                if (!clear) break;
+                len = m + 1;
+            }
+            if (len < k) len = 0;
+        } else {
+            bool ok = true;
+            for (u32 m = 0; m < k && ok; m++) {
+                const u64 x = p + (u64)m * (2 * k - 1 - m);
+                ok = is_prime_exact(x);
+                for (u64 y = x + 2; ok && m + 1 < k && y < x + 2 * (u64)(k - 1 - m); y += 2) ok = !is_prime_exact(y);
+            }
+            if (ok) {
+                len = k;
+                while (len < CS_MAXLEN) {
+                    const u64 gap = 2 * (u64)len;
+                    if (head < gap + 3) break;
+                    const u64 prev = head - gap;
+                    bool step = is_prime_exact(prev);
+                    for (u64 y = prev + 2; step && y < head; y += 2) step = !is_prime_exact(y);
+                    if (!step) break;
+                    head = prev;
+                    len++;
+                }
+            }
+        }
+        if (len) {
+            const ull j = atomicAdd(nres, 1ull);
+            if (j < cap) { heads[2 * j] = head; heads[2 * j + 1] = 0; lens[j] = len; }
+        }
+    }
+}
+
 // all the kernels of one unit of one shape, queued on st.  The survivors end in lists[*fin];
 // counters: cnt[0] the sieve's, cnt[r + 1] after screening round r, cnt[*fcnt] the final one.
 struct CsLists {
@@ -496,17 +544,27 @@ std::vector<u32> chain_offsets(u32 k, u32 shape)
 }
 
 // for the member offsets offs: the wheel (grown while W <= 3e7 and the classes number at most
-// 24,000), the pattern groups of the primes above it up to CS_PMAX (periods up to 2^24) and
+// 24,000), the pattern groups of the primes above it up to pattern_pmax (periods up to 2^24) and
 // their patterns.  False when some prime leaves no admissible residue: then no p at or above
 // CS_SIEVE_LO has all its members prime.
+// the largest pattern prime for patterns of k members: the screen's work falls with the
+// survivors, each further prime q removing about k/q of them, while every group costs a window
+// read per live word; short patterns leave many survivors and gain from deeper patterns
+u32 pattern_pmax(u32 k)
+{
+    return (k >= 6 && k < 12) ? CS_PMAX_LIMIT : 199u;
+}
+
 bool make_plan(const std::vector<u32> &offs, CsPlan &P)
 {
+    const u32 pmax = pattern_pmax((u32)offs.size());
+    static_assert(CS_PMAX_LIMIT < CS_SIEVE_LO, "members above CS_SIEVE_LO exceed every pattern prime");
     P.k = (u32)offs.size();
     P.offs = offs;
     std::vector<u64> cls{0};
     u64 W = 1;
     u32 q = 2;
-    for (; q <= CS_PMAX; q++) {
+    for (; q <= pmax; q++) {
         if (!is_small_prime(q)) continue;
         std::vector<u32> adm;
         for (u32 r = 0; r < q; r++) {
@@ -526,11 +584,11 @@ bool make_plan(const std::vector<u32> &offs, CsPlan &P)
     std::sort(cls.begin(), cls.end());
     P.W = W;
     P.res.assign(cls.begin(), cls.end());
-    // groups of the next primes up to CS_PMAX
+    // groups of the next primes up to pmax
     std::vector<std::vector<u32>> groups;
     std::vector<u32> cur;
     u64 per = 1;
-    for (; q <= CS_PMAX; q++) {
+    for (; q <= pmax; q++) {
         if (!is_small_prime(q)) continue;
         if (per * q > CS_PERIOD_MAX) { groups.push_back(cur); cur.clear(); per = 1; }
         cur.push_back(q);
@@ -579,7 +637,9 @@ void sort_chains(std::vector<u128t> &H, std::vector<u32> &L)
     if (n < 2) return;
     std::vector<u128t> h2(n);
     std::vector<u32> l2(n);
-    for (int sh = 0; sh < 128; sh += 11) {
+    u128t top = 0;
+    for (const u128t &v : H) top |= v;
+    for (int sh = 0; sh < 128 && (top >> sh); sh += 11) {
         std::vector<size_t> cnt(2048, 0);
         for (const u128t &v : H) cnt[(size_t)(v >> sh) & 2047]++;
         if (*std::max_element(cnt.begin(), cnt.end()) == n) continue;
@@ -762,8 +822,15 @@ static int cs_collect(mp_handle *h, ChainDev &D, const u64 *list, const ull *nin
     MP_CUDA(h, D.rl.ensure(cap * 4));
     MP_CUDA(h, cudaMemsetAsync(nres, 0, sizeof(ull), st));
     const u64 grid = std::max<u64>(1, std::min<u64>((expect + 127) / 128, (u64)h->sm_count * 16));
-    cs_verify_kernel<<<(unsigned)grid, 128, 0, st>>>(list, nin, cap, (u64)base, (u64)(base >> 64), D.k, D.mode,
-                                                     D.rh.as<u64>(), D.rl.as<u32>(), nres);
+    // one-word arithmetic when every candidate, member and interloper of the list stays below
+    // 2^64 - 2^12: a unit spans at most 256 segments of 2^17 W < 2^17 3e7 integers (below 2^50),
+    // and members and extensions lie within 2^11 of their candidate
+    if (base < ((u128t)1 << 64) - ((u128t)1 << 51))
+        cs_verify64_kernel<<<(unsigned)grid, 128, 0, st>>>(list, nin, cap, (u64)base, D.k, D.mode, D.rh.as<u64>(),
+                                                           D.rl.as<u32>(), nres);
+    else
+        cs_verify_kernel<<<(unsigned)grid, 128, 0, st>>>(list, nin, cap, (u64)base, (u64)(base >> 64), D.k, D.mode,
+                                                         D.rh.as<u64>(), D.rl.as<u32>(), nres);
     MP_CUDA(h, cudaGetLastError());
     ull nr = 0;
     MP_CUDA(h, cudaMemcpyAsync(&nr, nres, sizeof nr, cudaMemcpyDeviceToHost, st));
