@@ -32,6 +32,23 @@ def test_library_exports_the_gapsieve_interface():
     assert set(ENTRY) <= exported
 
 
+def test_interface_refuses_to_run_without_a_gpu():
+    """No CPU fallback: without a GPU, cu_init fails, and the reference's host then reports that
+    it cannot use the GPU (gapchain/gapsieve_cuda_host.c:91-92)."""
+    try:
+        import torch
+        if torch.cuda.is_available():
+            pytest.skip("a GPU is present")
+    except Exception:
+        pass
+    import ctypes as C
+    import mathpub_b200 as mp
+    L = mp.lib()
+    L.cu_init.argtypes = [C.c_char_p, C.c_size_t]
+    name = C.create_string_buffer(64)
+    assert L.cu_init(name, 64) != 0
+
+
 def sprp2(n):
     if n == 2:
         return True
