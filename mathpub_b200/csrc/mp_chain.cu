@@ -126,6 +126,8 @@ __device__ __forceinline__ bool member_sprp2(u64 base_lo, u64 base_hi, u64 off, 
 }
 
 // exact primality for any u64: trial division below 2^20, BPSW above (no pseudoprime below 2^64)
+// after trial division by the primes 3..61, which settles most of the odd numbers between the
+// members of a chain (those were never sieved) without an exponentiation
 __device__ bool is_prime_exact(u64 x)
 {
     if (x < 4) return x >= 2;
@@ -136,6 +138,10 @@ __device__ bool is_prime_exact(u64 x)
             if (y % d == 0) return false;
         return true;
     }
+    if (x % 3 == 0 || x % 5 == 0 || x % 7 == 0 || x % 11 == 0 || x % 13 == 0 || x % 17 == 0 || x % 19 == 0 ||
+        x % 23 == 0 || x % 29 == 0 || x % 31 == 0 || x % 37 == 0 || x % 41 == 0 || x % 43 == 0 || x % 47 == 0 ||
+        x % 53 == 0 || x % 59 == 0 || x % 61 == 0)
+        return false;
     return bpsw_odd(x);
 }
 
