@@ -207,6 +207,11 @@ int mp_chain_first128(mp_handle *h, const uint64_t lo[2], const uint64_t hi[2], 
 #define MP_TUPLE_MAXOFF 2048
 int mp_tuple_count(mp_handle *h, uint64_t lo, uint64_t hi, const uint32_t *offs, uint32_t k, uint64_t *count,
                    uint64_t *cks);
+/* the same for ranges above 2^64 (lo, hi as (low word, high word) pairs, hi <= 3.3e24, members
+ * above 2^64 certified by the 13 prime bases 2..41); the checksum term of p is the reference's
+ * hashp(p) = mix64(lo64(p) ^ hi64(p) * GOLD) (A350826/a350826.c:434-438), mix64(p) below 2^64 */
+int mp_tuple_count128(mp_handle *h, const uint64_t lo[2], const uint64_t hi[2], const uint32_t *offs, uint32_t k,
+                      uint64_t *count, uint64_t *cks);
 
 /* ---- BPSW ----
  * verdict bit i (bit i & 7 of byte i >> 3) = 1 iff n[i] is prime.  For n < 2^64 this is

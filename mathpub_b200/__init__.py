@@ -119,6 +119,7 @@ def lib():
             "mp_gap_chains": ([vp, u64, u64, u32, vp, vp, C.c_size_t, C.POINTER(C.c_size_t)], C.c_int),
             "mp_chain_sieve": ([vp, u64, u64, u32, u32, vp, vp, C.c_size_t, C.POINTER(C.c_size_t)], C.c_int),
             "mp_tuple_count": ([vp, u64, u64, vp, u32, C.POINTER(u64), C.POINTER(u64)], C.c_int),
+            "mp_tuple_count128": ([vp, vp, vp, vp, u32, C.POINTER(u64), C.POINTER(u64)], C.c_int),
             "mp_chain_first": ([vp, u64, u64, u32, u32, C.POINTER(u64), C.POINTER(u64), C.POINTER(u32)], C.c_int),
             "mp_chain_sieve128": ([vp, vp, vp, u32, u32, vp, vp, C.c_size_t, C.POINTER(C.c_size_t)], C.c_int),
             "mp_chain_first128": ([vp, vp, vp, u32, u32, vp, vp, C.POINTER(u32)], C.c_int),
@@ -333,6 +334,14 @@ class Engine:
         o = np.ascontiguousarray(offs, dtype=np.uint32)
         n, c = C.c_uint64(), C.c_uint64()
         self._check(lib().mp_tuple_count(self._h, lo, hi, _p(o), len(o), C.byref(n), C.byref(c)))
+        return n.value, c.value
+
+    def tuple_count128(self, lo, hi, offs):
+        """tuple_count for 128-bit ranges (mp_tuple_count128, hi <= 3.3e24): (count, checksum)."""
+        o = np.ascontiguousarray(offs, dtype=np.uint32)
+        wl, wh = self._w2(lo), self._w2(hi)
+        n, c = C.c_uint64(), C.c_uint64()
+        self._check(lib().mp_tuple_count128(self._h, _p(wl), _p(wh), _p(o), len(o), C.byref(n), C.byref(c)))
         return n.value, c.value
 
     def wieferich_range(self, lo, hi):

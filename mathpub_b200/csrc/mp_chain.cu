@@ -687,6 +687,25 @@ __global__ void __launch_bounds__(128) cs_tuple_kernel(const u64 *__restrict__ i
     }
 }
 
+// the same above 2^64: every member prime (13-base Miller-Rabin above 2^64), and the reference's
+// checksum term hashp(p) = mix64(lo64(p) xor hi64(p) GOLD) (A350826/a350826.c:434-438), which is
+// mix64(p) below 2^64
+__global__ void __launch_bounds__(128) cs_tuple128_kernel(const u64 *__restrict__ in, const ull *nin, u64 cap,
+                                                          u64 base_lo, u64 base_hi, const u32 *__restrict__ offs,
+                                                          u32 k, ull *acc)
+{
+    const u64 n = min((u64)*nin, cap);
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
+        const w2 p = w2_addu(w2{base_lo, base_hi}, in[i]);
+        bool ok = true;
+        for (u32 m = 0; m < k && ok; m++) ok = is_prime_w2(w2_addu(p, offs[m]));
+        if (ok) {
+            atomicAdd(acc, 1ull);
+            atomicAdd(acc + 1, (ull)mp_mix64(p.lo ^ (p.hi * MP_GOLD)));
+        }
+    }
+}
+
 // ---- mp_chain_sieve, mp_chain_first and mp_tuple_count: one plan and buffers per handle ----
 
 #define CS_MODE_TUPLE 2u                       // modes 0 and 1 are the chain shapes
@@ -1002,21 +1021,19 @@ extern "C" int mp_chain_first128(mp_handle *h, const uint64_t lo[2], const uint6
     return MP_OK;
 }
 
-extern "C" int mp_tuple_count(mp_handle *h, uint64_t lo, uint64_t hi, const uint32_t *offs, uint32_t k,
-                              uint64_t *count, uint64_t *cks)
+static int cs_tuple_check(mp_handle *h, const uint32_t *offs, uint32_t k)
 {
-    if (!h || !offs || !count || !cks) return MP_EINVAL;
-    *count = 0;
-    *cks = 0;
     if (k < 2 || k > MP_TUPLE_MAXK) return mp_set_error(h, MP_EINVAL, "k must be in 2..%d", MP_TUPLE_MAXK);
     if (offs[0] != 0) return mp_set_error(h, MP_EINVAL, "offs[0] must be 0");
     for (u32 i = 1; i < k; i++)
         if (offs[i] <= offs[i - 1] || (offs[i] & 1) || offs[i] > MP_TUPLE_MAXOFF)
             return mp_set_error(h, MP_EINVAL, "offsets must be even and increasing, at most %d", MP_TUPLE_MAXOFF);
-    if (hi > MP_CHAIN_SIEVE_HI_MAX) return mp_set_error(h, MP_ERANGE, "hi must be <= 2^64 - 2^12");
-    if (hi <= lo) return MP_OK;
-    std::lock_guard<std::recursive_mutex> lk(h->mu);
-    MP_CUDA(h, cudaSetDevice(h->device));
+    return MP_OK;
+}
+
+static int cs_tuples(mp_handle *h, u128t lo, u128t hi, const uint32_t *offs, uint32_t k, uint64_t *count,
+                     uint64_t *cks)
+{
     cudaStream_t st = h->stream;
     MP_TRY(cs_prepare(h, CS_MODE_TUPLE, std::vector<u32>(offs, offs + k)));
     ChainDev &D = *h->chain;
@@ -1026,7 +1043,12 @@ extern "C" int mp_tuple_count(mp_handle *h, uint64_t lo, uint64_t hi, const uint
         h, D, lo, hi, st,
         [&](const u64 *list, const ull *nin, u64 cap_, u128t base, u64 expect) {
             const u64 grid = std::max<u64>(1, std::min<u64>((expect + 127) / 128, (u64)h->sm_count * 16));
-            cs_tuple_kernel<<<(unsigned)grid, 128, 0, st>>>(list, nin, cap_, (u64)base, D.offs.as<u32>(), D.k, acc);
+            if (base < ((u128t)1 << 64) - ((u128t)1 << 51))          // every member below 2^64 - 2^12
+                cs_tuple_kernel<<<(unsigned)grid, 128, 0, st>>>(list, nin, cap_, (u64)base, D.offs.as<u32>(), D.k,
+                                                                acc);
+            else
+                cs_tuple128_kernel<<<(unsigned)grid, 128, 0, st>>>(list, nin, cap_, (u64)base, (u64)(base >> 64),
+                                                                   D.offs.as<u32>(), D.k, acc);
             return cudaGetLastError() == cudaSuccess ? MP_OK : mp_set_error(h, MP_ECUDA, "tuple kernel launch failed");
         },
         cs_never));
@@ -1036,6 +1058,35 @@ extern "C" int mp_tuple_count(mp_handle *h, uint64_t lo, uint64_t hi, const uint
     *count = r[0];
     *cks = r[1];
     return MP_OK;
+}
+
+extern "C" int mp_tuple_count(mp_handle *h, uint64_t lo, uint64_t hi, const uint32_t *offs, uint32_t k,
+                              uint64_t *count, uint64_t *cks)
+{
+    if (!h || !offs || !count || !cks) return MP_EINVAL;
+    *count = 0;
+    *cks = 0;
+    MP_TRY(cs_tuple_check(h, offs, k));
+    if (hi > MP_CHAIN_SIEVE_HI_MAX) return mp_set_error(h, MP_ERANGE, "hi must be <= 2^64 - 2^12");
+    if (hi <= lo) return MP_OK;
+    std::lock_guard<std::recursive_mutex> lk(h->mu);
+    MP_CUDA(h, cudaSetDevice(h->device));
+    return cs_tuples(h, lo, hi, offs, k, count, cks);
+}
+
+extern "C" int mp_tuple_count128(mp_handle *h, const uint64_t lo[2], const uint64_t hi[2], const uint32_t *offs,
+                                 uint32_t k, uint64_t *count, uint64_t *cks)
+{
+    if (!h || !lo || !hi || !offs || !count || !cks) return MP_EINVAL;
+    *count = 0;
+    *cks = 0;
+    MP_TRY(cs_tuple_check(h, offs, k));
+    const u128t L0 = (u128t)lo[1] << 64 | lo[0], H0 = (u128t)hi[1] << 64 | hi[0];
+    if (H0 > CS_HI128_MAX) return mp_set_error(h, MP_ERANGE, "hi must be <= 3.3e24");
+    if (H0 <= L0) return MP_OK;
+    std::lock_guard<std::recursive_mutex> lk(h->mu);
+    MP_CUDA(h, cudaSetDevice(h->device));
+    return cs_tuples(h, L0, H0, offs, k, count, cks);
 }
 
 // ---- the cu_* interface of gapchain/gapsieve_cuda.h ----
