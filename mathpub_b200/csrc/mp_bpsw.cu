@@ -1,25 +1,23 @@
-// mp_bpsw.cu -- 64-bit Montgomery BPSW primality test for B200 (sm_100a).
+// mp_bpsw.cu -- 64-bit BPSW primality test for B200 (sm_100a): batches of candidate lists.
 //
-// Reference (paths inside the Mathpub project): inv64/mmul64/madd64/msub64/mhalf64
-// A350826/a350826.c:565-604, sprp2_64 :618-638, jacobi :693, selfridge :739, slprp64
-// :766-799, bpsw :965-969, and the breadth-first batching of test_batch64 :1392.
-//
-// Differences in method, not in results:
-//   - R mod n (the Montgomery form of 1) is computed by doubling 2^(bitlen(n)-1) up to 2^64
-//     (exact; no division and no floating-point estimate), and the forms of Q and D by
-//     double-and-add of that one;
-//   - trial division by the odd primes up to 127 uses the multiplicative-inverse test
-//     (q | n iff n * q^-1 mod 2^64 <= (2^64 - 1) / q, for odd q) before any exponentiation;
-//   - perfect squares are rejected with an exact integer square root.
-// The verdict is primality for every n < 2^64 (BPSW has no pseudoprime below 2^64).
+// Reference (paths inside the Mathpub project): bpsw A350826/a350826.c:965 (the base-2 strong
+// test sprp2_64 :618 and the strong Lucas test slprp64 :766 with Selfridge's D :739), after
+// the trivial small-factor handling of is_prime_ref :529; the breadth-first batching of
+// test_batch64 :1392.  The arithmetic and the two tests are in mp_mont64.cuh.  Trial division
+// by the odd primes up to 127 uses the multiplicative-inverse test (q | n iff n q^-1 mod 2^64
+// <= (2^64 - 1) / q, for odd q), all 30 of them for every candidate, with no early exit.  The
+// verdict is primality for every n < 2^64 (BPSW has no pseudoprime below 2^64).
 //
 // Two launch structures:
 //   plain    one launch per candidate list, one thread per candidate, all phases inline;
-//   batched  one persistent launch over every list: warps pop chunks of 1024 candidates from
-//            a device work queue, trial-divide, compact the survivors with warp ballots, run
-//            the base-2 test on them, compact the passers, run the Lucas test, and write the
-//            verdict words.  Compaction keeps the lanes on uniform work; warps never wait for
-//            one another.
+//   batched  one persistent launch over every list: warps pop chunks of candidates from a
+//            device work queue, trial-divide them, and file the survivors in two classes by
+//            size: below 2^62 (from the front of a shared-memory list; these run the lazy
+//            Montgomery products) and above (from the back).  Each class runs the base-2 test
+//            in batches of 32 that are uniform in kind and nearly so in exponent length, the
+//            passers are compacted with warp ballots, the Lucas test runs on them, and the
+//            warp writes the chunk's verdict words.  Warps never wait for one another.  The
+//            warps per CTA and candidates per chunk are picked by the autotuner.
 #include "mp_mont64.cuh"
 
 #define TD_N 30            // odd primes 3..127
@@ -33,20 +31,18 @@ __constant__ u64 c_small_prime_mask[2];   // bit n set iff n < 128 is prime
 __device__ __forceinline__ int td_verdict(u64 n)
 {
     if (n < 128) return (int)((c_small_prime_mask[n >> 6] >> (n & 63)) & 1);
-    if (!(n & 1)) return 0;
+    bool f = !(n & 1);
 #pragma unroll
-    for (int k = 0; k < TD_N; k++)
-        if (n * c_td_inv[k] <= c_td_lim[k]) return 0;
-    if (n < 131ull * 131ull) return 1;
-    return -1;
+    for (int k = 0; k < TD_N; k++) f |= n * c_td_inv[k] <= c_td_lim[k];
+    if (f) return 0;
+    return n < 131ull * 131ull ? 1 : -1;
 }
 
 __device__ __forceinline__ bool bpsw_full(u64 n)
 {
     const int v = td_verdict(n);
     if (v >= 0) return v != 0;
-    const u64 ni = m_inv(n), one = m_one(n);
-    return sprp2_dev(n, ni, one) && slprp_dev(n, ni, one);
+    return bpsw_odd(n);
 }
 
 // ---- plain form: one thread per candidate of one list ----
@@ -60,20 +56,20 @@ __global__ void __launch_bounds__(256) bpsw_plain_kernel(const u64 *__restrict__
 }
 
 // ---- batched form: persistent warps over chunks of the concatenated lists ----
-// Each warp pops chunks of BPSW_WCHUNK candidates from the device work queue and runs the
-// three phases on them with ballot compaction in between, so its lanes stay on uniform work;
-// warps never wait for each other (no CTA barrier).
-#define BPSW_WCHUNK 1024
-#define BPSW_WARPS 8
+// a work-queue chunk is BPSW_WCHUNK candidates per warp, BPSW_WARPS warps per CTA; the
+// autotuner picks among the instantiated pairs (bpsw_batched_launch)
+#define BPSW_LAZY_MAX (1ull << 62)
 
+template <int BPSW_WARPS, int BPSW_WCHUNK>
 __global__ void __launch_bounds__(BPSW_WARPS * 32) bpsw_batched_kernel(const u64 *__restrict__ n, u64 total,
                                                                        u32 *__restrict__ bits, u32 *queue)
 {
-    __shared__ u16 s_idx[BPSW_WARPS][BPSW_WCHUNK];
+    __shared__ u16 s_idx[BPSW_WARPS][BPSW_WCHUNK];   // survivors: < 2^62 from the front, >= 2^62 from the back
+    __shared__ u16 s_pas[BPSW_WARPS][BPSW_WCHUNK];   // base-2 passers
     __shared__ u32 s_bits[BPSW_WARPS][BPSW_WCHUNK / 32];
     const u32 lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const u32 lt = (1u << lane) - 1;
-    u16 *idx = s_idx[warp];
+    u16 *idx = s_idx[warp], *pas = s_pas[warp];
     u32 *wb = s_bits[warp];
     const u64 nchunks = (total + BPSW_WCHUNK - 1) / BPSW_WCHUNK;
     for (;;) {
@@ -84,42 +80,47 @@ __global__ void __launch_bounds__(BPSW_WARPS * 32) bpsw_batched_kernel(const u64
         const u64 c0 = (u64)c * BPSW_WCHUNK;
         const u32 len = (u32)(total - c0 < BPSW_WCHUNK ? total - c0 : BPSW_WCHUNK);
         const u64 *nc = n + c0;
-        // 1. trial division; verdict words for the decided candidates, survivors compacted
-        u32 ns = 0;
+        // 1. trial division: verdict words of the decided candidates; survivors filed by class
+        u32 ns = 0, nl = 0;
         for (u32 base = 0; base < len; base += 32) {
             const u32 i = base + lane;
             const u64 x = i < len ? __ldg(nc + i) : 0;
             const int v = i < len ? td_verdict(x) : 0;
             const u32 pm = __ballot_sync(0xffffffffu, v == 1);
-            const u32 um = __ballot_sync(0xffffffffu, v < 0);
+            const bool sm = v < 0 && x < BPSW_LAZY_MAX, lg = v < 0 && x >= BPSW_LAZY_MAX;
+            const u32 ms = __ballot_sync(0xffffffffu, sm), ml = __ballot_sync(0xffffffffu, lg);
             if (lane == 0) wb[base >> 5] = pm;
-            if (v < 0) idx[ns + __popc(um & lt)] = (u16)i;
-            ns += __popc(um);
+            if (sm) idx[ns + __popc(ms & lt)] = (u16)i;
+            if (lg) idx[BPSW_WCHUNK - 1 - (nl + __popc(ml & lt))] = (u16)i;
+            ns += __popc(ms);
+            nl += __popc(ml);
         }
         __syncwarp();
-        // 2. base-2 strong test on the survivors; passers compacted to the front of idx
-        u32 nl = 0;
+        // 2. base-2 strong test, one class after the other; passers compacted into pas
+        u32 np = 0;
         for (u32 base = 0; base < ns; base += 32) {
             const u32 k = base + lane;
-            const bool act = k < ns;
-            const u32 i = act ? idx[k] : 0;
-            bool pass = false;
-            if (act) {
-                const u64 x = __ldg(nc + i);
-                pass = sprp2_dev(x, m_inv(x), m_one(x));
-            }
-            const u32 m = __ballot_sync(0xffffffffu, pass);   // every lane has read idx[k]
-            if (pass) idx[nl + __popc(m & lt)] = (u16)i;
-            nl += __popc(m);
-            __syncwarp();
+            const u32 i = k < ns ? idx[k] : 0;
+            const bool pass = k < ns && spsp2<true>(mm_setup(__ldg(nc + i)));
+            const u32 m = __ballot_sync(0xffffffffu, pass);
+            if (pass) pas[np + __popc(m & lt)] = (u16)i;
+            np += __popc(m);
         }
-        // 3. strong Lucas test on the base-2 passers
         for (u32 base = 0; base < nl; base += 32) {
             const u32 k = base + lane;
-            if (k < nl) {
-                const u32 i = idx[k];
-                const u64 x = __ldg(nc + i);
-                if (slprp_dev(x, m_inv(x), m_one(x))) atomicOr(&wb[i >> 5], 1u << (i & 31));
+            const u32 i = k < nl ? idx[BPSW_WCHUNK - 1 - k] : 0;
+            const bool pass = k < nl && spsp2<false>(mm_setup(__ldg(nc + i)));
+            const u32 m = __ballot_sync(0xffffffffu, pass);
+            if (pass) pas[np + __popc(m & lt)] = (u16)i;
+            np += __popc(m);
+        }
+        __syncwarp();
+        // 3. strong Lucas test on the base-2 passers
+        for (u32 base = 0; base < np; base += 32) {
+            const u32 k = base + lane;
+            if (k < np) {
+                const u32 i = pas[k];
+                if (lucas_u64(__ldg(nc + i))) atomicOr(&wb[i >> 5], 1u << (i & 31));
             }
         }
         __syncwarp();
@@ -141,9 +142,7 @@ static int bpsw_consts(mp_handle *h)
     u64 inv[TD_N], lim[TD_N], mask[2] = {0, 0};
     for (int k = 0; k < TD_N; k++) {
         const u64 q = tdp[k];
-        u64 x = (3 * q) ^ 2;
-        for (int i = 0; i < 4; i++) x *= 2 - q * x;
-        inv[k] = x;
+        inv[k] = inv64(q);
         lim[k] = ~0ull / q;
     }
     for (u32 v = 2; v < 128; v++) {
@@ -156,6 +155,23 @@ static int bpsw_consts(mp_handle *h)
     MP_CUDA(h, cudaMemcpyToSymbol(c_small_prime_mask, mask, sizeof mask));
     if (h->device >= 0 && h->device < 16) g_bpsw_consts[h->device] = true;
     return MP_OK;
+}
+
+// one persistent launch: as many CTAs as fit on the device, no more than the chunks need
+template <int WARPS, int CHUNK>
+static cudaError_t bpsw_batched_launch(mp_handle *h, const u64 *d_n, u64 total, u32 *d_bits, cudaStream_t st)
+{
+    int per_sm = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bpsw_batched_kernel<WARPS, CHUNK>,
+                                                                  WARPS * 32, 0);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) per_sm = 1;
+    u64 grid = (u64)h->sm_count * per_sm;
+    const u64 nchunks = (total + CHUNK - 1) / CHUNK;
+    const u64 need = (nchunks + WARPS - 1) / WARPS;
+    if (grid > need) grid = need;
+    bpsw_batched_kernel<WARPS, CHUNK><<<(unsigned)grid, WARPS * 32, 0, st>>>(d_n, total, d_bits, h->queue.as<u32>());
+    return cudaGetLastError();
 }
 
 // lists at d_n + offs[i] (offs multiples of 32, host array of nlists + 1 entries), verdict
@@ -178,15 +194,19 @@ int mp_bpsw_run(mp_handle *h, const u64 *d_n, const u64 *offs, const u32 *lens, 
     if (!total) return MP_OK;
     MP_CUDA(h, h->queue.ensure(64));
     MP_CUDA(h, cudaMemsetAsync(h->queue.p, 0, 4, st));
-    int per_sm = 0;
-    MP_CUDA(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bpsw_batched_kernel, BPSW_WARPS * 32, 0));
-    if (per_sm < 1) per_sm = 1;
-    u64 grid = (u64)h->sm_count * per_sm;
-    const u64 nchunks = (total + BPSW_WCHUNK - 1) / BPSW_WCHUNK;
-    const u64 need = (nchunks + BPSW_WARPS - 1) / BPSW_WARPS;
-    if (grid > need) grid = need;
     ProfScope ps(h, PROF_BPSW_BATCHED, st);
-    bpsw_batched_kernel<<<(unsigned)grid, BPSW_WARPS * 32, 0, st>>>(d_n, total, d_bits, h->queue.as<u32>());
-    MP_CUDA(h, cudaGetLastError());
+    switch (h->tune.bpsw_variant) {
+    case 1: MP_CUDA(h, (bpsw_batched_launch<4, 1024>(h, d_n, total, d_bits, st))); break;
+    case 2: MP_CUDA(h, (bpsw_batched_launch<8, 512>(h, d_n, total, d_bits, st))); break;
+    case 3: MP_CUDA(h, (bpsw_batched_launch<16, 512>(h, d_n, total, d_bits, st))); break;
+    default: MP_CUDA(h, (bpsw_batched_launch<8, 1024>(h, d_n, total, d_bits, st))); break;
+    }
     return MP_OK;
+}
+
+const char *mp_bpsw_variant_name(int v)
+{
+    static const char *names[4] = {"8 warps x 1024 candidates", "4 warps x 1024 candidates",
+                                   "8 warps x 512 candidates", "16 warps x 512 candidates"};
+    return names[v & 3];
 }

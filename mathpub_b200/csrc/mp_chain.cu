@@ -85,7 +85,7 @@ __device__ __forceinline__ w2 w2_mmul(w2 a, w2 b, w2 n, u64 ni)
 // the base-2 strong probable-prime test, odd 3 <= n < 2^127
 __device__ bool sprp2_w2(w2 n)
 {
-    const u64 ni = 0 - m_inv(n.lo);
+    const u64 ni = 0 - inv64(n.lo);
     // 1 in Montgomery form, 2^128 mod n, by doubling 2^b (b = the top bit of n, so 2^b < n)
     const int b = n.hi ? 127 - __clzll((long long)n.hi) : 63 - __clzll((long long)n.lo);
     w2 one = b >= 64 ? w2{0, 1ull << (b - 64)} : w2{1ull << b, 0};
@@ -121,7 +121,7 @@ __device__ __forceinline__ bool member_sprp2(u64 base_lo, u64 base_hi, u64 off, 
     const u64 l2 = lo + o;
     hi += l2 < lo;
     lo = l2;
-    if (!hi) return sprp2_dev(lo, m_inv(lo), m_one(lo));
+    if (!hi) return spsp2_u64(lo);
     return sprp2_w2(w2{lo, hi});
 }
 
@@ -180,7 +180,7 @@ __device__ bool is_prime_w2(w2 n)
         const u64 q = B[i], t = (~0ull % q + 1) % q;
         if (((n.hi % q) * t + n.lo % q) % q == 0) return false;
     }
-    const u64 ni = 0 - m_inv(n.lo);
+    const u64 ni = 0 - inv64(n.lo);
     const int b = 127 - __clzll((long long)n.hi);
     w2 one = w2{0, 1ull << (b - 64)};
     for (int i = b; i < 128; i++) one = w2_madd(one, one, n);

@@ -168,6 +168,7 @@ struct Autotune {
     int sieve_tile_log2 = 0;         // 0 = not tuned
     int sieve_threads = 0;
     int fermat_variant = 0;
+    int bpsw_variant = 0;            // warps per CTA x candidates per chunk of the batched BPSW kernel
     u64 tuned_at = 0;
 };
 
@@ -292,6 +293,7 @@ int mp_sieve_emit_primes(mp_handle *h, u64 lo, u64 hi, u64 *d_primes, u64 cap, u
 int mp_sieve_errors(mp_handle *h, cudaStream_t st);                  // synchronises; reads the error flag
 int mp_bpsw_run(mp_handle *h, const u64 *d_n, const u64 *offs, const u32 *lens, u32 nlists,
                 u32 *d_bits, u32 mode, cudaStream_t st);             // mp_bpsw.cu
+const char *mp_bpsw_variant_name(int v);
 int mp_fermat_run(mp_handle *h, const u64 *d_p, u64 count, u64 *d_q, cudaStream_t st,
                   int variant, u64 *d_partials);                     // mp_fermat.cu
 int mp_fermat_reduce(mp_handle *h, const u64 *d_p, const u64 *d_q, u64 count,

@@ -1,31 +1,39 @@
-// mp_mont64.cuh -- 64-bit Montgomery arithmetic (R = 2^64) and the two halves of BPSW: the
-// base-2 strong probable-prime test and the strong Lucas test with Selfridge's parameters.
-// Shared by the BPSW kernels (mp_bpsw.cu) and the constellation sieve (mp_chain.cu).
+// mp_mont64.cuh -- arithmetic modulo an odd 64-bit n, and the BPSW primality test built on it,
+// for B200 (sm_100a).  Used by the BPSW kernels (mp_bpsw.cu) and the constellation sieve
+// (mp_chain.cu).
 //
-// Reference (paths inside the Mathpub project): inv64/mmul64/madd64/msub64/mhalf64
-// A350826/a350826.c:565-604, sprp2_64 :618-638, jacobi :693, selfridge :739, slprp64
-// :766-799.  R mod n is found by doubling (exact; no floating-point estimate).
+// What is computed follows the reference (paths inside the Mathpub project): the base-2 strong
+// probable-prime test (sprp2_64, A350826/a350826.c:618), the strong Lucas test with Selfridge's
+// parameters (slprp64 :766, D from selfridge :739) and their conjunction (bpsw :965).  Both
+// give exact primality below 2^64, so the verdicts are the reference's.  How it is computed is
+// this file's own design, from the published mathematics:
+//
+//  * A residue is two 32-bit limbs.  A product is the full 128-bit product followed by a
+//    word-by-word Montgomery reduction (R = 2^64; per word m = t_i (-n^-1) mod 2^32, t += m n
+//    2^(32 i)), each one PTX block of 32-bit multiply-add carry chains.
+//  * For n < 2^62 (so 4n <= R) residues stay in [0, 2n) and no product is followed by a
+//    subtraction (lazy reduction).  Above, every product ends with one conditional subtraction
+//    (the 129-bit sum keeps its carry word, so every odd n < 2^64 is handled).
+//  * Base-2 exponentiation, left to right: square, then multiply by 2^b for the exponent bit b
+//    as a funnel shift of the residue by b (0 or 1) and one conditional subtraction; no select
+//    between two candidate residues.
+//  * Lucas sequences (P = 1, Q = (1 - D)/4) run as the ladder (V_k, V_k+1, Q^k) with
+//        V_2k = V_k^2 - 2 Q^k,   V_2k+1 = V_k V_k+1 - P Q^k,
+//    the same four products for either exponent bit (the bit only selects operands), so the
+//    lanes of a warp never diverge on the exponent.  U_d = 0 (mod n) is read off as
+//    2 V_d+1 = P V_d (mod n): D U_k = 2 V_k+1 - P V_k, and gcd(D, n) = 1 when (D/n) = -1.
+//  * The Jacobi symbol is the binary (shift and subtract) algorithm after one reduction n mod
+//    |D|; the perfect-square check (a square has no D with (D/n) = -1) runs only after 24 values
+//    of D have failed.
 #pragma once
 #include "mp_common.cuh"
 
-// ---- 64-bit Montgomery arithmetic, R = 2^64 ----
-
-__device__ __forceinline__ u64 m_mul(u64 a, u64 b, u64 n, u64 ni)
+// n^-1 mod 2^64 for odd n.  n n = 1 (mod 8), so n is its own inverse to 3 bits; each Newton
+// step x (2 - n x) doubles the correct bits: 6, 12, 24, 48, 96.
+__host__ __device__ __forceinline__ u64 inv64(u64 n)
 {
-    const u64 tl = a * b, th = __umul64hi(a, b);
-    const u64 m = tl * ni;
-    const u64 mh = __umul64hi(m, n);
-    const u64 r = th - mh;
-    return th < mh ? r + n : r;
-}
-__device__ __forceinline__ u64 m_add(u64 a, u64 b, u64 n) { const u64 s = a + b; return (s < a || s >= n) ? s - n : s; }
-__device__ __forceinline__ u64 m_sub(u64 a, u64 b, u64 n) { return a >= b ? a - b : a - b + n; }
-__device__ __forceinline__ u64 m_half(u64 a, u64 n) { return (a & 1) ? (a >> 1) + (n >> 1) + 1 : a >> 1; }
-
-// n^-1 mod 2^64 for odd n: (3n) xor 2 is correct to 5 bits; four Newton steps give 80
-__device__ __forceinline__ u64 m_inv(u64 n)
-{
-    u64 x = (3 * n) ^ 2;
+    u64 x = n;
+    x *= 2 - n * x;
     x *= 2 - n * x;
     x *= 2 - n * x;
     x *= 2 - n * x;
@@ -33,149 +41,362 @@ __device__ __forceinline__ u64 m_inv(u64 n)
     return x;
 }
 
-// 2^64 mod n for odd n > 1, by doubling 2^b (b = top bit of n, so 2^b < n) 64 - b times
-__device__ __forceinline__ u64 m_one(u64 n)
-{
-    const int b = 63 - __clzll((long long)n);
-    u64 x = 1ull << b;
-    for (int i = b; i < 64; i++) x = m_add(x, x, n);
-    return x;
-}
+// the modulus with what the products need: its limbs, -n^-1 mod 2^32, 2n, and R mod n
+struct Mod64 {
+    u64 n, n2;     // n and 2n (2n is used below 2^62 only)
+    u64 one;       // R mod n, the residue of 1
+    u32 np;        // -n^-1 mod 2^32
+};
 
-// Montgomery form of a small signed integer v (|v| < n) by double-and-add of `one`
-__device__ __forceinline__ u64 m_small(i32 v, u64 one, u64 n)
+// ---- products: t = a b (128 bits), then t += m0 n + m1 n 2^32, result t / 2^64 ----
+
+// the reduction tail shared by the products: t0..t3 hold a b; leaves the result in t2, t3 and
+// its carry word in t4 (0 or 1)
+#define MM_REDUCE_FULL                                   \
+    "mul.lo.u32     m, t0, %3;\n\t"                      \
+    "mad.lo.cc.u32  t0, m, n0, t0;\n\t"                  \
+    "madc.lo.cc.u32 t1, m, n1, t1;\n\t"                  \
+    "addc.cc.u32    t2, t2, 0;\n\t"                      \
+    "addc.cc.u32    t3, t3, 0;\n\t"                      \
+    "addc.u32       t4, 0, 0;\n\t"                       \
+    "mad.hi.cc.u32  t1, m, n0, t1;\n\t"                  \
+    "madc.hi.cc.u32 t2, m, n1, t2;\n\t"                  \
+    "addc.cc.u32    t3, t3, 0;\n\t"                      \
+    "addc.u32       t4, t4, 0;\n\t"                      \
+    "mul.lo.u32     m, t1, %3;\n\t"                      \
+    "mad.lo.cc.u32  t1, m, n0, t1;\n\t"                  \
+    "madc.lo.cc.u32 t2, m, n1, t2;\n\t"                  \
+    "addc.cc.u32    t3, t3, 0;\n\t"                      \
+    "addc.u32       t4, t4, 0;\n\t"                      \
+    "mad.hi.cc.u32  t2, m, n0, t2;\n\t"                  \
+    "madc.hi.cc.u32 t3, m, n1, t3;\n\t"                  \
+    "addc.u32       t4, t4, 0;\n\t"                      \
+    /* the result is below 2n: subtract n once when it is >= n (bw = 0) */ \
+    "sub.cc.u32     d0, t2, n0;\n\t"                     \
+    "subc.cc.u32    d1, t3, n1;\n\t"                     \
+    "subc.u32       bw, t4, 0;\n\t"                      \
+    "setp.ne.u32    p, bw, 0;\n\t"                       \
+    "selp.u32       t2, t2, d0, p;\n\t"                  \
+    "selp.u32       t3, t3, d1, p;\n\t"
+
+// n < 2^62: every partial sum stays below 2^128 (a b < 4n^2 <= 2^126), so no carry word, and
+// the result (below 2n) is not reduced
+#define MM_REDUCE_LAZY                                   \
+    "mul.lo.u32     m, t0, %3;\n\t"                      \
+    "mad.lo.cc.u32  t0, m, n0, t0;\n\t"                  \
+    "madc.lo.cc.u32 t1, m, n1, t1;\n\t"                  \
+    "addc.cc.u32    t2, t2, 0;\n\t"                      \
+    "addc.u32       t3, t3, 0;\n\t"                      \
+    "mad.hi.cc.u32  t1, m, n0, t1;\n\t"                  \
+    "madc.hi.cc.u32 t2, m, n1, t2;\n\t"                  \
+    "addc.u32       t3, t3, 0;\n\t"                      \
+    "mul.lo.u32     m, t1, %3;\n\t"                      \
+    "mad.lo.cc.u32  t1, m, n0, t1;\n\t"                  \
+    "madc.lo.cc.u32 t2, m, n1, t2;\n\t"                  \
+    "addc.u32       t3, t3, 0;\n\t"                      \
+    "mad.hi.cc.u32  t2, m, n0, t2;\n\t"                  \
+    "madc.hi.u32    t3, m, n1, t3;\n\t"
+
+#define MM_REGS ".reg .u32 a0, a1, b0, b1, n0, n1, t0, t1, t2, t3, t4, m, d0, d1, bw;\n\t.reg .pred p;\n\t"
+
+// a^2 / R mod n.  LAZY (n < 2^62): a in [0, 2n), result in [0, 2n).  Otherwise a in [0, n),
+// result in [0, n).
+template <bool LAZY>
+__device__ __forceinline__ u64 mm_sqr(u64 a, const Mod64 &M)
 {
-    u32 a = v < 0 ? (u32)(-v) : (u32)v;
-    u64 r = 0;
-    for (int i = 31 - __clz((int)(a | 1)); i >= 0; i--) {
-        r = m_add(r, r, n);
-        if ((a >> i) & 1) r = m_add(r, one, n);
-    }
-    if (v < 0 && r) r = n - r;
+    u64 r;
+    if (LAZY)
+        asm("{\n\t" MM_REGS
+            "mov.b64 {a0, a1}, %1;\n\t"
+            "mov.b64 {n0, n1}, %2;\n\t"
+            "mul.lo.u32     t0, a0, a0;\n\t"
+            "mul.hi.u32     t1, a0, a0;\n\t"
+            "mul.lo.u32     t2, a1, a1;\n\t"
+            "mul.hi.u32     t3, a1, a1;\n\t"
+            "mad.lo.cc.u32  t1, a0, a1, t1;\n\t"
+            "madc.hi.cc.u32 t2, a0, a1, t2;\n\t"
+            "addc.u32       t3, t3, 0;\n\t"
+            "mad.lo.cc.u32  t1, a0, a1, t1;\n\t"
+            "madc.hi.cc.u32 t2, a0, a1, t2;\n\t"
+            "addc.u32       t3, t3, 0;\n\t"
+            MM_REDUCE_LAZY
+            "mov.b64 %0, {t2, t3};\n\t}"
+            : "=l"(r) : "l"(a), "l"(M.n), "r"(M.np));
+    else
+        asm("{\n\t" MM_REGS
+            "mov.b64 {a0, a1}, %1;\n\t"
+            "mov.b64 {n0, n1}, %2;\n\t"
+            "mul.lo.u32     t0, a0, a0;\n\t"
+            "mul.hi.u32     t1, a0, a0;\n\t"
+            "mul.lo.u32     t2, a1, a1;\n\t"
+            "mul.hi.u32     t3, a1, a1;\n\t"
+            "mad.lo.cc.u32  t1, a0, a1, t1;\n\t"
+            "madc.hi.cc.u32 t2, a0, a1, t2;\n\t"
+            "addc.u32       t3, t3, 0;\n\t"
+            "mad.lo.cc.u32  t1, a0, a1, t1;\n\t"
+            "madc.hi.cc.u32 t2, a0, a1, t2;\n\t"
+            "addc.u32       t3, t3, 0;\n\t"
+            MM_REDUCE_FULL
+            "mov.b64 %0, {t2, t3};\n\t}"
+            : "=l"(r) : "l"(a), "l"(M.n), "r"(M.np));
     return r;
 }
 
-// ---- base-2 strong probable-prime test (odd n > 2) ----
-__device__ __forceinline__ bool sprp2_dev(u64 n, u64 ni, u64 one)
+// a b / R mod n for a, b in [0, n), result in [0, n)
+__device__ __forceinline__ u64 mm_mul(u64 a, u64 b, const Mod64 &M)
 {
-    const u64 mone = n - one;
-    u64 d = n - 1;
-    const int s = __ffsll((long long)d) - 1;
-    d >>= s;
-    const int top = 63 - __clzll((long long)d);
-    u64 x = m_add(one, one, n);                  // 2, for the top bit of d
-    for (int i = top - 1; i >= 0; i--) {
-        x = m_mul(x, x, n, ni);
-        const u64 y = m_add(x, x, n);
-        x = ((d >> i) & 1) ? y : x;
+    u64 r;
+    asm("{\n\t" MM_REGS
+        "mov.b64 {a0, a1}, %1;\n\t"
+        "mov.b64 {n0, n1}, %2;\n\t"
+        "mov.b64 {b0, b1}, %4;\n\t"
+        "mul.lo.u32     t0, a0, b0;\n\t"
+        "mul.hi.u32     t1, a0, b0;\n\t"
+        "mul.lo.u32     t2, a1, b1;\n\t"
+        "mul.hi.u32     t3, a1, b1;\n\t"
+        "mad.lo.cc.u32  t1, a0, b1, t1;\n\t"
+        "madc.hi.cc.u32 t2, a0, b1, t2;\n\t"
+        "addc.u32       t3, t3, 0;\n\t"
+        "mad.lo.cc.u32  t1, a1, b0, t1;\n\t"
+        "madc.hi.cc.u32 t2, a1, b0, t2;\n\t"
+        "addc.u32       t3, t3, 0;\n\t"
+        MM_REDUCE_FULL
+        "mov.b64 %0, {t2, t3};\n\t}"
+        : "=l"(r) : "l"(a), "l"(M.n), "r"(M.np), "l"(b));
+    return r;
+}
+
+// x 2^b mod n for b in {0, 1}: a funnel shift by b, then one conditional subtraction.
+// LAZY (n < 2^62): x in [0, 2n), subtracts 2n, result in [0, 2n).  Otherwise x in [0, n), the
+// bit shifted out of 64 is kept, result in [0, n).
+template <bool LAZY>
+__device__ __forceinline__ u64 mm_dbl(u64 x, u32 b, const Mod64 &M)
+{
+    u64 r;
+    if (LAZY)
+        asm("{\n\t.reg .u32 x0, x1, n0, n1, y0, y1, d0, d1, bw;\n\t.reg .pred p;\n\t"
+            "mov.b64 {x0, x1}, %1;\n\t"
+            "mov.b64 {n0, n1}, %2;\n\t"
+            "shl.b32         y0, x0, %3;\n\t"
+            "shf.l.clamp.b32 y1, x0, x1, %3;\n\t"
+            "sub.cc.u32      d0, y0, n0;\n\t"
+            "subc.cc.u32     d1, y1, n1;\n\t"
+            "subc.u32        bw, 0, 0;\n\t"
+            "setp.ne.u32     p, bw, 0;\n\t"
+            "selp.u32        y0, y0, d0, p;\n\t"
+            "selp.u32        y1, y1, d1, p;\n\t"
+            "mov.b64 %0, {y0, y1};\n\t}"
+            : "=l"(r) : "l"(x), "l"(M.n2), "r"(b));
+    else
+        asm("{\n\t.reg .u32 x0, x1, n0, n1, y0, y1, c, d0, d1, bw;\n\t.reg .pred p;\n\t"
+            "mov.b64 {x0, x1}, %1;\n\t"
+            "mov.b64 {n0, n1}, %2;\n\t"
+            "shl.b32         y0, x0, %3;\n\t"
+            "shf.l.clamp.b32 y1, x0, x1, %3;\n\t"
+            "shr.b32         c, x1, 31;\n\t"
+            "and.b32         c, c, %3;\n\t"
+            "sub.cc.u32      d0, y0, n0;\n\t"
+            "subc.cc.u32     d1, y1, n1;\n\t"
+            "subc.u32        bw, c, 0;\n\t"
+            "setp.ne.u32     p, bw, 0;\n\t"
+            "selp.u32        y0, y0, d0, p;\n\t"
+            "selp.u32        y1, y1, d1, p;\n\t"
+            "mov.b64 %0, {y0, y1};\n\t}"
+            : "=l"(r) : "l"(x), "l"(M.n), "r"(b));
+    return r;
+}
+
+// (a + b) mod n and (a - b) mod n for a, b in [0, n)
+__device__ __forceinline__ u64 mm_add(u64 a, u64 b, u64 n)
+{
+    const u64 s = a + b;
+    const u64 t = s - n;
+    // a + b >= n exactly when the sum wrapped past 2^64 or the difference did not borrow
+    return (s < a || s >= n) ? t : s;
+}
+__device__ __forceinline__ u64 mm_sub(u64 a, u64 b, u64 n)
+{
+    const u64 d = a - b;
+    return a < b ? d + n : d;
+}
+
+// [0, 2n) -> [0, n)
+__device__ __forceinline__ u64 mm_canon(u64 x, u64 n) { return x >= n ? x - n : x; }
+
+// the modulus set-up: -n^-1 mod 2^32 and R mod n.  R mod n = 2^64 mod n is reached from
+// 2^(bitlen(n) - 1) < n by doublings, which are exact.
+__device__ __forceinline__ Mod64 mm_setup(u64 n)
+{
+    Mod64 M;
+    M.n = n;
+    M.n2 = n << 1;
+    M.np = 0u - (u32)inv64(n);
+    const int top = 63 - __clzll((long long)n);
+    u64 x = 1ull << top;
+    for (int i = top; i < 64; i++) x = mm_dbl<false>(x, 1u, M);
+    M.one = x;
+    return M;
+}
+
+// Montgomery residue of a small signed integer v (|v| < n): |v| R by double-and-add of R mod n
+// over the bits of |v|, then negated
+__device__ __forceinline__ u64 mm_from_small(i32 v, const Mod64 &M)
+{
+    const u32 a = v < 0 ? (u32)(-v) : (u32)v;
+    u64 r = 0;
+    for (int i = 31 - __clz(a | 1u); i >= 0; i--) {
+        r = mm_dbl<false>(r, 1u, M);
+        if ((a >> i) & 1u) r = mm_add(r, M.one, M.n);
     }
-    if (x == one || x == mone) return true;
-    for (int i = 1; i < s; i++) {
-        x = m_mul(x, x, n, ni);
-        if (x == mone) return true;
-        if (x == one) return false;
+    return (v < 0 && r) ? M.n - r : r;
+}
+
+// ---- base-2 strong probable-prime test ----
+
+// n - 1 = d 2^s with d odd: 2^d (mod n) by the left-to-right ladder, then the strong
+// condition 2^d = 1, or 2^(d 2^r) = -1 for some 0 <= r < s.  Odd n > 2.
+template <bool LAZY>
+__device__ __forceinline__ bool spsp2(const Mod64 &M)
+{
+    const u64 n = M.n;
+    const int s = __ffsll((long long)(n - 1)) - 1;
+    const u64 d = (n - 1) >> s;
+    const int L = 63 - __clzll((long long)d);               // d's top bit: the ladder starts at 2
+    u64 x = mm_dbl<false>(M.one, 1u, M);
+    for (int i = L - 1; i >= 0; i--) {
+        x = mm_sqr<LAZY>(x, M);
+        x = mm_dbl<LAZY>(x, (u32)(d >> i) & 1u, M);
     }
-    return false;
+    const u64 mone = n - M.one;                             // the residue of -1
+    if (LAZY) x = mm_canon(x, n);
+    bool pass = x == M.one || x == mone;
+    for (int r = 1; r < s && !pass; r++) {
+        if (x == M.one) break;                              // 1 before -1: not a strong probable prime
+        x = mm_sqr<LAZY>(x, M);
+        if (LAZY) x = mm_canon(x, n);
+        pass = x == mone;
+    }
+    return pass;
+}
+
+// the test for any odd n > 2, with the lazy form chosen by size
+__device__ __forceinline__ bool spsp2_u64(u64 n)
+{
+    const Mod64 M = mm_setup(n);
+    return n < (1ull << 62) ? spsp2<true>(M) : spsp2<false>(M);
 }
 
 // ---- strong Lucas test ----
 
-// Jacobi symbol (D/n) for odd D with |D| < n, odd n
-__device__ __forceinline__ int jacobi_small(i32 D, u64 n)
+// Jacobi symbol (a/m) for odd m > 0 and 0 <= a < m: strip factors 2 of a (each flips the sign
+// when m = 3, 5 mod 8), swap by reciprocity when a < m (flip when a = m = 3 mod 4), subtract
+__device__ __forceinline__ int jacobi32(u32 a, u32 m)
 {
     int t = 1;
-    u32 a;
-    if (D < 0) {
-        a = (u32)(-D);
-        if ((n & 3) == 3) t = -t;             // (-1/n)
-    } else a = (u32)D;
-    if ((a & 3) == 3 && (n & 3) == 3) t = -t; // reciprocity (a/n) = +-(n/a), a odd
-    u32 x = (u32)(n % a), m = a;
-    while (x) {
-        while (!(x & 1)) {
-            x >>= 1;
-            const u32 r = m & 7;
-            if (r == 3 || r == 5) t = -t;
+    while (a) {
+        const int z = __ffs((int)a) - 1;
+        a >>= z;
+        if ((z & 1) && ((m & 7u) == 3u || (m & 7u) == 5u)) t = -t;
+        if (a < m) {
+            const u32 x = a;
+            a = m;
+            m = x;
+            if (a & m & 2u) t = -t;
         }
-        const u32 tmp = x; x = m; m = tmp;
-        if ((x & 3) == 3 && (m & 3) == 3) t = -t;
-        x %= m;
+        a -= m;
     }
     return m == 1 ? t : 0;
 }
 
-__device__ __forceinline__ u64 isqrt_dev(u64 n)
+// (D/n) for odd n > |D|, D odd: (-1/n) for the sign, then reciprocity (|D|/n) = +-(n mod |D| / |D|)
+__device__ __forceinline__ int jacobi_dn(i32 D, u64 n)
 {
-    u64 r = 0, bit = 1ull << 62;
-    while (bit > n) bit >>= 2;
-    while (bit) {
-        if (n >= r + bit) { n -= r + bit; r = (r >> 1) + bit; }
-        else r >>= 1;
-        bit >>= 2;
-    }
-    return r;
+    const u32 a = D < 0 ? (u32)(-D) : (u32)D;
+    int t = 1;
+    if (D < 0 && (n & 3) == 3) t = -t;
+    if ((a & 3u) == 3u && (n & 3) == 3) t = -t;
+    return t * jacobi32((u32)(n % a), a);
 }
 
-__device__ __forceinline__ bool is_square_dev(u64 n)
+// exact test for a perfect square: residue filters mod 64 and 63, then the integer root by
+// bits from the top
+__device__ __forceinline__ bool is_square64(u64 n)
 {
-    // squares mod 64 are 0, 1, 4, 9, 16, 17, 25, 33, 36, 41, 49, 57
-    const u64 sq64 = (1ull << 0) | (1ull << 1) | (1ull << 4) | (1ull << 9) | (1ull << 16) | (1ull << 17) |
-                     (1ull << 25) | (1ull << 33) | (1ull << 36) | (1ull << 41) | (1ull << 49) | (1ull << 57);
-    if (!((sq64 >> (n & 63)) & 1)) return false;
-    const u64 r = isqrt_dev(n);
+    if (!((0x0202021202030213ull >> (n & 63)) & 1)) return false;
+    if (!((0x0402483012450293ull >> (n % 63)) & 1)) return false;
+    u64 r = 0;
+    for (int b = 31; b >= 0; b--) {
+        const u64 c = r | (1ull << b);
+        if (c * c <= n) r = c;
+    }
     return r * r == n;
 }
 
-// Selfridge method A: first D in 5, -7, 9, -11, ... with (D/n) = -1.  The search is bounded;
-// for n < 2^64 that is not a square a suitable D has |D| far below the bound.
-__device__ __forceinline__ bool selfridge_dev(u64 n, i32 *Dout)
+// Selfridge's method A: the first D of 5, -7, 9, -11, 13, ... with (D/n) = -1.  Returns 0 when
+// n is shown composite on the way: some |D| < n shares a factor with n, or n is a perfect
+// square (no D exists then).  Odd n, larger than the |D| reached.
+__device__ __forceinline__ i32 selfridge_d(u64 n)
 {
-    if (is_square_dev(n)) return false;
-    i32 D = 5;
-    for (int it = 0; it < 4096; it++) {
-        const int j = jacobi_small(D, n);
-        if (j == -1) { *Dout = D; return true; }
-        if (j == 0 && (u64)(D < 0 ? -D : D) != n) return false;
-        D = D > 0 ? -(D + 2) : -(D - 2);
+    for (int k = 0; k < 2048; k++) {
+        const i32 a = 5 + 2 * k;
+        const i32 D = (k & 1) ? -a : a;
+        const int j = jacobi_dn(D, n);
+        if (j < 0) return D;
+        if (j == 0 && (u64)a != n) return 0;
+        if (k == 23 && is_square64(n)) return 0;
     }
-    return false;
+    return 0;
 }
 
-__device__ __forceinline__ bool slprp_dev(u64 n, u64 ni, u64 one)
+// strong Lucas probable prime with P = 1, Q = (1 - D)/4 (D = 1 mod 4 here, so Q is exact):
+// n + 1 = d 2^s, d odd; U_d = 0, or V_(d 2^r) = 0 for some 0 <= r < s.  Odd n > 2, n < 2^64 - 1.
+__device__ __forceinline__ bool lucas_strong(const Mod64 &M, i32 D)
 {
-    i32 D;
-    if (!selfridge_dev(n, &D)) return false;
+    const u64 n = M.n;
     const i32 Q = (1 - D) / 4;
-    const u64 Qm = m_small(Q, one, n), Dm = m_small(D, one, n);
-    u64 d = n + 1;                               // n < 2^64 - 1 here (2^64 - 1 has factor 3)
-    const int s = __ffsll((long long)d) - 1;
-    d >>= s;
-    u64 U = one, V = one, Qk = Qm;
-    for (int b = 62 - __clzll((long long)d); b >= 0; b--) {
-        U = m_mul(U, V, n, ni);
-        V = m_sub(m_mul(V, V, n, ni), m_add(Qk, Qk, n), n);
-        Qk = m_mul(Qk, Qk, n, ni);
-        if ((d >> b) & 1) {
-            const u64 U2 = m_add(U, V, n);
-            const u64 V2 = m_add(m_mul(Dm, U, n, ni), V, n);
-            U = m_half(U2, n);
-            V = m_half(V2, n);
-            Qk = m_mul(Qk, Qm, n, ni);
-        }
+    const u64 q1 = mm_from_small(Q, M);
+    const int s = __ffsll((long long)(n + 1)) - 1;
+    const u64 d = (n + 1) >> s;
+    // k = 1 (d's top bit): V_1 = P = 1, V_2 = P^2 - 2Q, Q^1
+    u64 vk = M.one;
+    u64 vk1 = mm_sub(M.one, mm_add(q1, q1, n), n);
+    u64 qk = q1;
+    for (int i = 62 - __clzll((long long)d); i >= 0; i--) {
+        const bool b = (d >> i) & 1;
+        const u64 w = mm_sub(mm_mul(vk, vk1, M), qk, n);               // V_2k+1
+        const u64 qb = mm_mul(qk, b ? q1 : M.one, M);                  // Q^(k+b)
+        const u64 sq = mm_sqr<false>(b ? vk1 : vk, M);
+        const u64 v2 = mm_sub(sq, mm_add(qb, qb, n), n);               // V_2(k+b)
+        qk = mm_mul(qk, qb, M);                                        // Q^(2k+b)
+        vk = b ? w : v2;
+        vk1 = b ? v2 : w;
     }
-    if (U == 0 || V == 0) return true;
+    if (vk == 0 || mm_add(vk1, vk1, n) == vk) return true;             // V_d = 0 or U_d = 0
     for (int r = 1; r < s; r++) {
-        V = m_sub(m_mul(V, V, n, ni), m_add(Qk, Qk, n), n);
-        if (V == 0) return true;
-        Qk = m_mul(Qk, Qk, n, ni);
+        vk = mm_sub(mm_sqr<false>(vk, M), mm_add(qk, qk, n), n);        // V_(d 2^r)
+        if (vk == 0) return true;
+        qk = mm_sqr<false>(qk, M);
     }
     return false;
 }
 
-// primality of an odd n > 2 without small factors to look for first: the base-2 strong test
-// and the strong Lucas test (BPSW; exact for n < 2^64)
+// the Lucas half of BPSW for an odd n > 2 that passed the base-2 test
+__device__ __forceinline__ bool lucas_u64(u64 n)
+{
+    if (n == ~0ull) return false;                                      // 3 | 2^64 - 1
+    const i32 D = selfridge_d(n);
+    if (!D) return false;
+    return lucas_strong(mm_setup(n), D);
+}
+
+// primality of an odd n > 2 with no small factor to look for first: the base-2 strong test and
+// the strong Lucas test (BPSW; exact below 2^64)
 __device__ __forceinline__ bool bpsw_odd(u64 n)
 {
-    const u64 ni = m_inv(n), one = m_one(n);
-    return sprp2_dev(n, ni, one) && slprp_dev(n, ni, one);
+    if (n == ~0ull) return false;
+    const Mod64 M = mm_setup(n);
+    const bool p2 = n < (1ull << 62) ? spsp2<true>(M) : spsp2<false>(M);
+    if (!p2) return false;
+    const i32 D = selfridge_d(n);
+    return D && lucas_strong(M, D);
 }
