@@ -88,8 +88,15 @@ typedef struct {
 
 typedef mp_range_stats mp_block_stats;
 
-#define MP_MODE_BATCHED 0   /* persistent tile kernel + device work queue + CUDA graph */
-#define MP_MODE_PLAIN   1   /* one launch per segment (the reference's per-segment loop) */
+/* MP_MODE_BATCHED: the range in waves of tiles; per wave a bucket scatter for the large
+ *   primes, then a tile launch in which each CTA sieves a contiguous run of tiles and carries
+ *   the state of its sparse primes from tile to tile; the whole call is captured once as a
+ *   CUDA graph and replayed.
+ * MP_MODE_PLAIN: the reference's per-segment launch loop on a full grid: one launch per group
+ *   of SM-count 32 KiB segments, one segment per CTA, every segment set up from scratch,
+ *   each group with its own bucket scatter; no graph. */
+#define MP_MODE_BATCHED 0
+#define MP_MODE_PLAIN   1
 
 typedef struct {
     uint32_t mode;          /* MP_MODE_BATCHED (default) or MP_MODE_PLAIN */
@@ -251,7 +258,8 @@ int mp_fermat_q_base2_dev(mp_handle *h, const uint64_t *d_p, size_t count, uint6
  *   cks           sum of mix64(q ^ (p * 0x9E3779B97F4A7C15)) mod 2^64 (the reference's
  *                 checksum, A001220/wieferich.c:1064)
  *   ordered_hash  H <- H * 0x100000001b3 + mix64(p ^ mix64(q)) (mod 2^64) in p order
- *   hits          the Wieferich primes (q = 0) found, nhits of them (first 16 stored) */
+ *   hits          the Wieferich primes (q = 0): the smallest min(nhits, 16) of the nhits found,
+ *                 in increasing order; the other slots are 0 */
 typedef struct {
     uint64_t primes, tests, near, flt, cks, ordered_hash, nhits;
     uint64_t hits[16];
@@ -268,7 +276,11 @@ int mp_wieferich_range(mp_handle *h, uint64_t lo, uint64_t hi, mp_wief_stats *ou
  * the library that every device holds until exit and that all calls on a device share:
  * calls that overlap on the GPU race.  count above MP_NOALLOC_MAX_COUNT is refused with
  * MP_EINVAL.  The first call on a device looks up the array's device address; make that
- * call before any stream capture.  This entry point has no counterpart in the reference. */
+ * call before any stream capture.  The address is kept for the life of the process, so a
+ * device reset (cudaDeviceReset) between calls is not supported.  A CUDA error already
+ * pending in the calling thread is left for the caller and the call returns MP_ECUDA
+ * without running; an error from this call's own launches is cleared and returned as
+ * MP_ECUDA.  This entry point has no counterpart in the reference. */
 #define MP_NOALLOC_MAX_COUNT (1u << 24)
 int mp_wieferich_stats_noalloc(const uint64_t *d_p, const uint64_t *d_q, uint64_t count,
                                mp_wief_stats *d_stats, void *stream);

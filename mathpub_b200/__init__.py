@@ -25,6 +25,9 @@ MP_OK, MP_EINVAL, MP_ENOMEM, MP_ECUDA, MP_ETIMEOUT, MP_EOVERFLOW, MP_ERANGE, MP_
 MODE_BATCHED, MODE_PLAIN = 0, 1
 _ERRNAMES = {-1: "EINVAL", -2: "ENOMEM", -3: "ECUDA", -4: "ETIMEOUT", -5: "EOVERFLOW", -6: "ERANGE", -7: "EAGAIN", -8: "EBUSY"}
 
+# largest count mp_wieferich_stats_noalloc accepts (MP_NOALLOC_MAX_COUNT in include/mathpub_gpu.h)
+NOALLOC_MAX_COUNT = 1 << 24
+
 STATS_FIELDS = ["pi", "twins", "max_gap", "gap_start", "tuple6", "tuple6_cks", "first_prime", "last_prime"]
 WIEF_FIELDS = ["primes", "tests", "near", "flt", "cks", "ordered_hash", "nhits"]
 

@@ -379,8 +379,6 @@ int mp_wieferich_range(mp_handle *h, uint64_t lo, uint64_t hi, mp_wief_stats *ou
     float ms = 0;
     if (cudaEventElapsedTime(&ms, h->ev0, h->ev1) == cudaSuccess) h->last_ms = ms;
     out->primes = n;
-    const u64 nh = std::min<u64>(out->nhits, 16);
-    std::sort(out->hits, out->hits + nh);
     return MP_OK;
 }
 

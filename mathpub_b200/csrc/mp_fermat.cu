@@ -11,7 +11,9 @@
 // multiplied with the CIOS Montgomery product on 32x32->64 integer multiply-adds.  The form
 // of 1 (R mod N) is found by doubling 2^(bitlen(N)-1) up to R, exactly; the reference's
 // double-precision quotient estimates are not used.  The exponent p - 1 is processed left
-// to right: square, then double when the bit is 1 (base 2 needs no multiplier table).
+// to right: square, then double when the bit is 1 (base 2 needs no multiplier table).  Where
+// 8N < R (p < 2^46 with three limbs, p < 2^62 with four) the two are one product,
+// x (x 2^bit) / R, the doubling being a funnel shift of one operand.
 #include "mp_common.cuh"
 
 // t[0..K] += a[0..K-1] * b: the low halves of the products in one carry chain, then the high
@@ -168,15 +170,29 @@ __device__ __forceinline__ FermOut fermat_one(u64 p)
 #pragma unroll
     for (int j = 1; j < K; j++) n2[j] = (n[j] << 1) | (n[j - 1] >> 31);
     const u64 e = p - 1;
-    for (int b = 63 - __clzll((long long)e); b >= 0; b--) {
-        mmul_lazy<K>(x, x, x, n, np);
-        u32 y[K];
+    if (p < (K == 3 ? (1ull << 46) : (1ull << 62))) {
+        // 8N < R: the doubling for a 1 bit goes into the product.  x (x 2^bit) / R with
+        // x < 2N and x 2^bit < 4N (a funnel shift, no subtraction) is below
+        // (8N^2 + R N) / R < 2N, so the square-and-double of one bit is one product
+        for (int b = 63 - __clzll((long long)e); b >= 0; b--) {
+            const u32 bit = (u32)(e >> b) & 1u;
+            u32 y[K];
+            y[0] = x[0] << bit;
 #pragma unroll
-        for (int j = 0; j < K; j++) y[j] = x[j];
-        mdbl<K>(y, n2);
-        const bool bit = (e >> b) & 1;
+            for (int j = 1; j < K; j++) y[j] = __funnelshift_l(x[j - 1], x[j], bit);
+            mmul_lazy<K>(x, x, y, n, np);
+        }
+    } else {
+        for (int b = 63 - __clzll((long long)e); b >= 0; b--) {
+            mmul_lazy<K>(x, x, x, n, np);
+            u32 y[K];
 #pragma unroll
-        for (int j = 0; j < K; j++) x[j] = bit ? y[j] : x[j];
+            for (int j = 0; j < K; j++) y[j] = x[j];
+            mdbl<K>(y, n2);
+            const bool bit = (e >> b) & 1;
+#pragma unroll
+            for (int j = 0; j < K; j++) x[j] = bit ? y[j] : x[j];
+        }
     }
     // leave Montgomery form: multiply by 1; with x < 2N the product (x + mN) / R is at most N,
     // and mmul's subtraction brings it to [0, N)
@@ -267,8 +283,15 @@ __global__ void __launch_bounds__(FS_THREADS) fermat_stats_kernel(const u64 *__r
         f.h = f.h * MP_FNV_PRIME + mp_mix64(p ^ mp_mix64(q));
         f.len++;
         if (q == 0) {
-            const u64 k = atomicAdd((unsigned long long *)nhits, 1ull);
-            if (k < 16) hits[k] = p;
+            // keep the 16 smallest hits, sorted, whatever the order the threads arrive in:
+            // slot j keeps the smaller of its value and the incoming one and passes the larger
+            // on, so slot j ends with the (j+1)-th smallest value that ever reached it
+            atomicAdd((unsigned long long *)nhits, 1ull);
+            u64 v = p;
+            for (int j = 0; j < 16 && v != ~0ull; j++) {
+                const u64 old = atomicMin((unsigned long long *)(hits + j), (unsigned long long)v);
+                v = old > v ? old : v;
+            }
         }
     }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -311,7 +334,7 @@ __global__ void __launch_bounds__(1024) fermat_final_kernel(const FermPart *part
         out->cks = g.cks;
         out->ordered_hash = g.h;
         out->nhits = *nhits;
-        for (int k = 0; k < 16; k++) out->hits[k] = k < (int)*nhits ? hits[k] : 0;
+        for (int k = 0; k < 16; k++) out->hits[k] = (u64)k < *nhits ? hits[k] : 0;
     }
 }
 
@@ -342,7 +365,8 @@ int mp_fermat_reduce(mp_handle *h, const u64 *d_p, const u64 *d_q, u64 count, mp
     FermPart *parts = h->ferm_part.as<FermPart>();
     u64 *hits = (u64 *)((char *)h->ferm_part.p + nb * sizeof(FermPart));
     u64 *nhits = hits + 16;
-    MP_CUDA(h, cudaMemsetAsync(hits, 0, 17 * 8, st));
+    MP_CUDA(h, cudaMemsetAsync(hits, 0xff, 16 * 8, st));        // empty slots hold 2^64 - 1
+    MP_CUDA(h, cudaMemsetAsync(nhits, 0, 8, st));
     if (count) {
         ProfScope ps(h, PROF_FERMAT_STATS, st);
         fermat_stats_kernel<<<(unsigned)nb, FS_THREADS, 0, st>>>(d_p, d_q, count, parts, hits, nhits);
@@ -365,8 +389,9 @@ int mp_fermat_reduce(mp_handle *h, const u64 *d_p, const u64 *d_q, u64 count, mp
 // array below, which every GPU that loads this library keeps until the process exits.
 // ---------------------------------------------------------------------------------------
 
-#define NOALLOC_MAX_COUNT (1u << 24)                       // primes per call
-#define NOALLOC_PARTS (NOALLOC_MAX_COUNT / FS_TILE)       // one partial per CTA
+#define NOALLOC_PARTS (MP_NOALLOC_MAX_COUNT / FS_TILE)    // one partial per stats CTA
+static_assert(MP_NOALLOC_MAX_COUNT % FS_TILE == 0, "the scratch limit must be whole stats tiles");
+static_assert((u64)NOALLOC_PARTS * FS_TILE >= MP_NOALLOC_MAX_COUNT, "one partial per CTA of the largest call");
 
 struct NoallocScratch {
     FermPart parts[NOALLOC_PARTS];                          // 384 KB
@@ -377,35 +402,28 @@ struct NoallocScratch {
 static __device__ __align__(256) NoallocScratch g_noalloc_scratch;
 
 // The host sees g_noalloc_scratch only as a stand-in symbol: its device address is looked up
-// once per device with cudaGetSymbolAddress (with that device current) and kept here.
+// once per device with cudaGetSymbolAddress (with that device current) and kept here.  A
+// device reset between calls would move the array; that is not supported.
 static std::mutex g_noalloc_mu;
 static void *g_noalloc_ptr[64] = {nullptr};
 
+// the hit list and its count carry over from the previous call: empty slots hold 2^64 - 1
 __global__ void noalloc_clear_kernel(NoallocScratch *s)
 {
-    if (threadIdx.x < 16) s->hits[threadIdx.x] = 0;
+    if (threadIdx.x < 16) s->hits[threadIdx.x] = ~0ull;
     if (threadIdx.x == 0) s->nhits = 0;
 }
 
-// the entry count, and the stored hits in increasing order (the order in which the device
-// found them is arbitrary)
-__global__ void noalloc_finish_kernel(mp_wief_stats *out, u64 count)
-{
-    out->primes = count;
-    const int n = out->nhits < 16 ? (int)out->nhits : 16;
-    for (int i = 1; i < n; i++) {
-        const u64 v = out->hits[i];
-        int k = i - 1;
-        while (k >= 0 && out->hits[k] > v) { out->hits[k + 1] = out->hits[k]; k--; }
-        out->hits[k + 1] = v;
-    }
-}
+__global__ void noalloc_count_kernel(mp_wief_stats *out, u64 count) { out->primes = count; }
 
 extern "C" int mp_wieferich_stats_noalloc(const uint64_t *d_p, const uint64_t *d_q, uint64_t count,
                                            mp_wief_stats *d_stats, void *stream)
 {
     if (!d_stats || (count && (!d_p || !d_q))) return MP_EINVAL;
-    if (count > NOALLOC_MAX_COUNT) return MP_EINVAL;       // beyond the fixed scratch
+    if (count > MP_NOALLOC_MAX_COUNT) return MP_EINVAL;    // beyond the fixed scratch
+    // an error already pending in this thread belongs to the caller: leave it for the caller
+    // to read, and run nothing
+    if (cudaPeekAtLastError() != cudaSuccess) return MP_ECUDA;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return MP_ECUDA;
     NoallocScratch *s = nullptr;
@@ -413,21 +431,34 @@ extern "C" int mp_wieferich_stats_noalloc(const uint64_t *d_p, const uint64_t *d
         std::lock_guard<std::mutex> lk(g_noalloc_mu);
         if (!g_noalloc_ptr[dev]) {
             void *p = nullptr;
-            if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return MP_ECUDA;
+            if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) {
+                cudaGetLastError();                          // this call's own failure
+                return MP_ECUDA;
+            }
             g_noalloc_ptr[dev] = p;
         }
         s = (NoallocScratch *)g_noalloc_ptr[dev];
     }
     cudaStream_t st = (cudaStream_t)stream;
-    // the hit list carries over from the previous call: it must start at zero
+    // every launch is checked; a failure here is this call's own, so it is cleared
+#define NOALLOC_CHECK()                                                                       \
+    do {                                                                                      \
+        if (cudaPeekAtLastError() != cudaSuccess) { cudaGetLastError(); return MP_ECUDA; }   \
+    } while (0)
     noalloc_clear_kernel<<<1, 32, 0, st>>>(s);
+    NOALLOC_CHECK();
     const u64 nb = count ? (count + FS_TILE - 1) / FS_TILE : 0;
-    if (count) fermat_stats_kernel<<<(unsigned)nb, FS_THREADS, 0, st>>>(d_p, d_q, count, s->parts, s->hits, &s->nhits);
-    else {
-        // no input: one empty partial
-        if (cudaMemsetAsync(s->parts, 0, sizeof(FermPart), st) != cudaSuccess) return MP_ECUDA;
+    if (count) {
+        fermat_stats_kernel<<<(unsigned)nb, FS_THREADS, 0, st>>>(d_p, d_q, count, s->parts, s->hits, &s->nhits);
+        NOALLOC_CHECK();
+    } else if (cudaMemsetAsync(s->parts, 0, sizeof(FermPart), st) != cudaSuccess) {
+        cudaGetLastError();
+        return MP_ECUDA;                                     // no input: one empty partial
     }
     fermat_final_kernel<<<1, 1024, 0, st>>>(s->parts, nb ? nb : 1, &s->nhits, s->hits, d_stats);
-    noalloc_finish_kernel<<<1, 1, 0, st>>>(d_stats, count);
-    return cudaGetLastError() == cudaSuccess ? MP_OK : MP_ECUDA;
+    NOALLOC_CHECK();
+    noalloc_count_kernel<<<1, 1, 0, st>>>(d_stats, count);
+    NOALLOC_CHECK();
+#undef NOALLOC_CHECK
+    return MP_OK;
 }

@@ -1248,28 +1248,30 @@ static int scatter_bounds(mp_handle *h, const PrimeTable &tb, u32 i0, u32 i1, cu
     return MP_OK;
 }
 
-// mode: 0 batched (waves of tile launches, each CTA a contiguous run of tiles), 1 plain (one
-// launch per tile)
+// mode: 0 batched (waves of tile launches, each CTA a contiguous run of tiles), 1 plain (the
+// reference's per-segment launch loop on a full grid: one launch per group of sm_count
+// segments, one segment per CTA, each set up from scratch, with its own bucket scatter)
 static int run_tiles(mp_handle *h, const PrimeTable &tb, const SievePlan &P, TileArgs a, int mode, int emit,
                      cudaStream_t st)
 {
     const int nth = P.nth;
-    const u32 nlaunch = mode == 1 ? P.g.ntiles : P.nwaves;
+    const u32 plain_w = (u32)std::max(1, h->sm_count);
+    const u32 nlaunch = mode == 1 ? (P.g.ntiles + plain_w - 1) / plain_w : P.nwaves;
     const int grid_pers = h->sm_count * tile_ctas_per_sm(P.g.tlog, nth);
     // carried state of the sparse thread-tier primes: one slot per prime per CTA (written and
     // read by the tile kernel only; nothing needs clearing)
     MP_CUDA(h, h->tstate.ensure((size_t)grid_pers * (P.ti.it1 - P.ti.itd) * 4 + 64));
     a.tstate = h->tstate.as<u32>();
     u32 *errp = h->errflag.as<u32>();
+    const u32 wmax = mode == 1 ? std::min(plain_w, P.g.ntiles) : P.wt;
     if (P.large) {
-        const u32 wt = mode == 1 ? 1 : P.wt;
-        MP_CUDA(h, h->rec.ensure((size_t)wt * P.cap * 4));
-        MP_CUDA(h, h->reccnt.ensure((size_t)wt * 4 * 2));
+        MP_CUDA(h, h->rec.ensure((size_t)wmax * P.cap * 4));
+        MP_CUDA(h, h->reccnt.ensure((size_t)wmax * 4 * 2));
     }
     if (P.large) MP_TRY(scatter_bounds(h, tb, P.ti.it1, P.ti.iend, st));
     for (u32 L = 0; L < nlaunch; L++) {
-        const u32 t0 = mode == 1 ? L : L * P.wt;
-        const u32 nt = mode == 1 ? 1 : std::min(P.wt, P.g.ntiles - t0);
+        const u32 t0 = L * wmax;
+        const u32 nt = std::min(wmax, P.g.ntiles - t0);
         if (P.large) {
             ScatterArgs s;
             s.base = P.g.base; s.tlog = P.g.tlog; s.t0 = t0; s.wt = nt; s.nbx = P.g.nbx;
@@ -1285,7 +1287,7 @@ static int run_tiles(mp_handle *h, const PrimeTable &tb, const SievePlan &P, Til
             a.rec = s.rec; a.reccnt = s.cnt; a.reccap = P.cap;
         }
         a.t0 = t0; a.nt = nt;
-        const int grid = mode == 1 ? 1 : (int)std::min<u64>((u64)grid_pers, nt);
+        const int grid = mode == 1 ? (int)nt : (int)std::min<u64>((u64)grid_pers, nt);
         ProfScope ps(h, PROF_TILE, st);
         MP_CUDA(h, launch_tile_any(a, grid, nth, emit, st));
     }

@@ -33,9 +33,16 @@ def test_library_builds_and_exports_every_symbol():
     exported = set(re.findall(r"\bT (mp_[a-z0-9_]+)\b", out))
     missing = [f for f in declared_functions() if f not in exported]
     assert not missing, missing
-    # the compiled code is sm_100a only
-    cu = subprocess.run(["/usr/local/cuda/bin/cuobjdump", "--list-elf", lib], capture_output=True, text=True)
-    assert "sm_100a" in cu.stdout
+    # the build compiles for sm_100a only: one -gencode, for the B200
+    gencodes = [build.FLAGS[i + 1] for i, f in enumerate(build.FLAGS) if f == "-gencode"]
+    assert gencodes == ["arch=compute_100a,code=sm_100a"]
+
+
+def test_python_constants_match_the_header():
+    import mathpub_b200 as mp
+    src = open(os.path.join(ROOT, "include", "mathpub_gpu.h")).read()
+    m = re.search(r"#define MP_NOALLOC_MAX_COUNT \(1u << (\d+)\)", src)
+    assert m and mp.NOALLOC_MAX_COUNT == 1 << int(m.group(1))
 
 
 def test_library_loads_and_fails_loudly_without_gpu():
