@@ -19,8 +19,11 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_A350826 = os.path.join(HERE, "_ref", "libref_a350826.so")
+REF_A007508 = os.path.join(HERE, "_ref", "libref_a007508.so")
 REF_WIEFERICH = os.path.join(HERE, "_ref", "libref_wieferich.so")
-REFERENCE_TREE = "/root/reference"
+# the reference tree (read only to build the checkers): $MATHPUB_REFERENCE, else its checkout on
+# the build machine
+REFERENCE_TREE = os.environ.get("MATHPUB_REFERENCE", "/root/reference")
 
 STATS_FIELDS = ["pi", "twins", "max_gap", "gap_start", "tuple6", "tuple6_cks", "first_prime", "last_prime"]
 STATS_DTYPE = np.dtype([(n, np.uint64) for n in STATS_FIELDS])
@@ -42,7 +45,7 @@ class Wief(C.Structure):
 def build(ref=True):
     """Compile liboracle.so, and the reference checkers when the reference tree exists."""
     target = "ref" if ref and os.path.isdir(REFERENCE_TREE) else "all"
-    subprocess.run(["make", "-s", "-C", HERE, target], check=True)
+    subprocess.run(["make", "-s", "-C", HERE, target, f"MATHPUB_REFERENCE={REFERENCE_TREE}"], check=True)
 
 
 _o = None
@@ -94,6 +97,31 @@ def ra():
             f.restype = res
         _ra = L
     return _ra
+
+
+_rt = None
+
+
+def have_ref_twins():
+    return os.path.exists(REF_A007508)
+
+
+def rt():
+    """the reference's own twin-class sieve (A007508/a007508.c count_twins_twin)"""
+    global _rt
+    if _rt is None:
+        L = C.CDLL(REF_A007508)
+        L.ref_twins_k.argtypes = [C.c_uint64, C.c_uint64, C.c_int]
+        L.ref_twins_k.restype = C.c_uint64
+        _rt = L
+    return _rt
+
+
+def ref_twins(lo, hi, nthreads=None):
+    """Twin pairs (p, p + 2) with lo <= p < hi by the reference's twin sieve; lo, hi multiples
+    of 30 and lo > 5 (its k-space: p = 30 k + 11, 17 or 29)."""
+    assert lo % 30 == 0 and hi % 30 == 0 and lo > 5
+    return int(rt().ref_twins_k(lo // 30, hi // 30, nthreads or threads()))
 
 
 def rw():

@@ -1,9 +1,9 @@
 """Run one workload between cudaProfilerStart/Stop, for `ncu --profile-from-start off`.
 
-    python -m mathpub_b200.profile_case sieve  [--lo 1e15] [--log2span 32] [--tile 20] [--threads 1024]
-    python -m mathpub_b200.profile_case bpsw   [--log2count 22]
-    python -m mathpub_b200.profile_case fermat [--lo 1e12] [--span 1e8]
-    python -m mathpub_b200.profile_case chain  [--lo 1e15] [--span 1e8] [--k 16] [--dec]
+    python profile_case.py sieve  [--lo 1e15] [--log2span 32] [--tile 20] [--threads 1024]
+    python profile_case.py bpsw   [--log2count 22]
+    python profile_case.py fermat [--lo 1e12] [--span 1e8]
+    python profile_case.py chain  [--lo 1e15] [--span 1e8] [--k 16] [--dec]
 
 The tables are built and every kernel runs once before the profiled region, so the capture
 holds only the steady-state launches of one call.
@@ -14,7 +14,7 @@ import sys
 
 import numpy as np
 
-sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
 import mathpub_b200 as mp  # noqa: E402
 
 

@@ -28,7 +28,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
-REF = "/root/reference"
+# the reference tree: $MATHPUB_REFERENCE, else its checkout on the machine that made the fixtures
+REF = os.environ.get("MATHPUB_REFERENCE", "/root/reference")
 
 import oracle  # noqa: E402
 

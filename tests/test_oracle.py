@@ -137,6 +137,15 @@ def test_oracle_matches_compiled_reference(orc):
     assert (w["primes"], w["cks"], f) == (p, k, 0)
 
 
+@pytest.mark.skipif("not __import__('oracle').have_ref_twins()")
+@pytest.mark.parametrize("lo,hi", [(990, 30 * 10 ** 6), (30 * 10 ** 9, 30 * 10 ** 9 + 3 * 10 ** 7),
+                                   (999999999999990, 999999999999990 + 6 * 10 ** 7)])
+def test_twins_match_reference_twin_sieve(orc, lo, hi):
+    """The oracle's twin counts equal those of the reference's own twin-class bucket sieve
+    (A007508/a007508.c count_twins_twin), built from the reference's source."""
+    assert orc.sieve_range(lo, hi)["twins"] == orc.ref_twins(lo, hi)
+
+
 def test_config_fixtures_consistent(configs):
     c2 = configs["config2"]
     assert (c2["stats"]["tuple6"], c2["stats"]["tuple6_cks"]) == (c2["reference_tuple6"]["count"],
