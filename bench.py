@@ -45,6 +45,8 @@ HBM_FALLBACK_GBS = 6650.0
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one tile-kernel launch (a wave
 # of 1184 tiles at 1e15), from an ncu capture of that launch
 TILE_TRAFFIC_BYTES = 597.8e6 + 293.2e6
+# the same for the persistent pipeline launch of one step (None until captured)
+PIPE_TRAFFIC_BYTES = None
 WORKLOAD = ("large-offset sieve [1e15, 1e15+2^34) per GPU, odd-only bitmap, sieving primes up to 31623048, "
             "wheel/pattern presieve 3..89, bucket sieve above the tile; outputs per-2^24-block pi, twins, "
             "6-tuples {0,4,6,10,12,16} with checksum, max gap + start, per-2^20 FNV-1a bitmap hashes")
@@ -122,6 +124,50 @@ def algorithmic_work(primes, lo, hi, tile_bits):
     m = (coprime_below(k1) - coprime_below(k0)).astype(np.float64)
     small = qi <= np.uint64(tile_bits)
     return float(m[small].sum()), float(m[~small].sum())
+
+
+def _bitlen64(x):
+    """bit length of each uint64 (0 for 0), exact: the two 32-bit halves go through float64"""
+    x = np.asarray(x, dtype=np.uint64)
+    hi = (x >> np.uint64(32)).astype(np.float64)
+    lo = (x & np.uint64(0xffffffff)).astype(np.float64)
+    bh = np.frexp(hi)[1].astype(np.int64)
+    bl = np.frexp(lo)[1].astype(np.int64)
+    return np.where(hi > 0, 32 + bh, bl)
+
+
+def _odd_part(x):
+    """x / 2^v2(x) for nonzero uint64 x"""
+    x = np.asarray(x, dtype=np.uint64)
+    low = x & (~x + np.uint64(1))
+    return x >> (_bitlen64(low) - 1).astype(np.uint64)
+
+
+TD_PRIMES = [3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37, 41, 43, 47, 53, 59, 61, 67, 71, 73, 79, 83, 89, 97, 101, 103,
+             107, 109, 113, 127]
+# 32-bit multiply or multiply-add instructions (the multiply pipe) in one Montgomery product:
+# two limbs, 8 for the product and 10 for the two reduction rows (mp_mont64.cuh); three limbs
+# of the Fermat kernel, three rows of 3 + 3 (a b_i) + 1 (m) + 3 + 3 (m N) (mp_fermat.cu)
+IMAD_PER_PRODUCT_BPSW = 18
+IMAD_PER_PRODUCT_FERMAT_K3 = 39
+
+
+def bpsw_products(n, prime_mask):
+    """Montgomery products of the BPSW kernels on the candidates n, counted exactly from the
+    inputs: the base-2 ladder of every candidate that trial division leaves (bitlen(d) - 1
+    squarings, n - 1 = d 2^s) and the Lucas ladder of every prime among them (four products per
+    step, bitlen(d') - 1 steps, n + 1 = d' 2^s').  The squarings of the strong chains after the
+    ladders and the set-up are left out, so this is a lower bound on the work."""
+    n = np.asarray(n, dtype=np.uint64)
+    surv = ((n & np.uint64(1)) == 1) & (n >= np.uint64(131 * 131))
+    for q in TD_PRIMES:
+        surv &= (n % np.uint64(q)) != 0
+    ns = n[surv]
+    sprp = int((_bitlen64(_odd_part(ns - np.uint64(1))) - 1).sum())
+    npr = n[surv & prime_mask]
+    npr = npr[npr != np.uint64(0xffffffffffffffff)]
+    lucas = 4 * int((_bitlen64(_odd_part(npr + np.uint64(1))) - 1).sum())
+    return sprp, lucas, int(surv.sum()), int(len(npr))
 
 
 def run_ours(args):
@@ -210,7 +256,7 @@ def run_ours(args):
 
     # e2e through the host API: outputs copied to host memory every step
     e2e_ms = []
-    for _ in range(max(2, min(args.steps, 5))):
+    for _ in range(args.steps):
         flush.zero_()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -284,11 +330,15 @@ def run_ours(args):
     plain_bits = db.cpu().numpy().view(np.uint32)
     bpsw_same = bool(np.array_equal(bpsw_bits, plain_bits))
     bpsw_primes = int(np.unpackbits(bpsw_bits.view(np.uint8)).sum())
+    pmask = np.unpackbits(bpsw_bits.view(np.uint8), bitorder="little")[:len(flat)].astype(bool)
+    sprp_products, lucas_products, bpsw_survivors, bpsw_lucas_n = bpsw_products(flat, pmask)
 
     peaks = e.probe_peaks()
     hbm, hbm_src = peaks_file()
 
-    fermat = run_fermat(e, world, rank, dev) if not args.quick else None
+    fermat = run_fermat(e, world, rank, dev, peaks["imad32"]) if not args.quick else None
+    config1 = run_config1(e, dev, stream, flush, peaks, args.steps) if rank == 0 else None
+    reference_gpu = run_reference_gpu() if (rank == 0 and world == 1 and not args.quick) else None
     chains = run_chains(e) if (rank == 0 and not args.quick) else None
     tuples = run_tuples(e) if (rank == 0 and not args.quick) else None
     serving = run_serving(e, args) if (rank == 0 and not args.quick and args.serve_requests) else None
@@ -301,12 +351,29 @@ def run_ours(args):
         m = re.search(r"sieve choice: tile 2\^(\d+)", tune_report)
         if m:
             tile_bits = 1 << int(m.group(1))
-        marks_small, marks_large = algorithmic_work(primes, lo, hi, tile_bits)
+        m = re.search(r"bucket threshold tile/(\d+)", tune_report.split("sieve choice")[-1])
+        bucket_div = int(m.group(1)) if m else 1
+        marks_small, marks_large = algorithmic_work(primes, lo, hi, tile_bits // bucket_div)
         ntiles = -(-((hi + (1 << 16) - lo) // 2) // tile_bits)
-        tile_bytes = (marks_large * 4 + ntiles * (tile_bits // 8)) / max(tile_launches, 1)
-        tile_avg_s = tile_ms / max(tile_launches, 1) / 1e3
-        achieved = tile_bytes / tile_avg_s / 1e9
-        smem_marks_rate = (marks_small + marks_large) / (tile_ms / 1e3)
+        pipe_launches, pipe_ms = prof.get("pipeline", (0, 0.0))
+        if pipe_launches:
+            # one persistent launch per step runs the scatter and the tiles: its bytes are the
+            # bucket records written and read back (4 B each way) and the bitmap written
+            kname, klaunches, kms = "sieve_pipeline_kernel", pipe_launches, pipe_ms
+            kbytes = (marks_large * 8 + ntiles * (tile_bits // 8)) / pipe_launches
+            ktraffic = PIPE_TRAFFIC_BYTES
+            knote = ("bytes = bucket records written and read (4 B each way per large-prime hit) + bitmap written; "
+                     "the persistent launch also runs the scatter, so the atomic rate below is over the whole step")
+        else:
+            kname, klaunches, kms = f"tile_kernel<{tile_bits.bit_length() - 1},0>", tile_launches, tile_ms
+            kbytes = (marks_large * 4 + ntiles * (tile_bits // 8)) / max(tile_launches, 1)
+            ktraffic = TILE_TRAFFIC_BYTES
+            knote = ("bytes = bucket records read (4 B per large-prime hit) + bitmap written; traffic = DRAM bytes of "
+                     "one launch from an ncu capture; the kernel is bound by instruction issue and shared-memory "
+                     "atomics, see roofline_smem")
+        tile_avg_s = kms / max(klaunches, 1) / 1e3
+        achieved = kbytes / tile_avg_s / 1e9
+        smem_marks_rate = (marks_small + marks_large) / (kms / 1e3)
         ref_fixture = None
         try:
             with open(os.path.join(ROOT, "tests", "golden", "configs.json")) as f:
@@ -326,13 +393,10 @@ def run_ours(args):
                     "api": "mp_sieve_range (host buffers)"},
             "gpu_launches": launches_per_step * args.steps,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                         "frac": achieved / hbm, "traffic": TILE_TRAFFIC_BYTES,
-                         "kernel": f"tile_kernel<{tile_bits.bit_length() - 1},0>",
+                         "frac": achieved / hbm, "traffic": ktraffic, "kernel": kname,
                          "peak_source": f"{hbm_src} (MEASURED_PEAKS.json hbm_gbs)" if hbm_src == "measured" else "fallback",
-                         "algorithmic_bytes_per_launch": tile_bytes, "avg_launch_ms": tile_avg_s * 1e3,
-                         "note": "bytes = bucket records read (4 B per large-prime hit) + bitmap written; traffic = "
-                                 "DRAM bytes of one launch from an ncu capture; the kernel is bound by instruction "
-                                 "issue and shared-memory atomics, see roofline_smem"},
+                         "algorithmic_bytes_per_launch": kbytes, "avg_launch_ms": tile_avg_s * 1e3,
+                         "bucket_threshold": tile_bits // bucket_div, "note": knote},
             "roofline_smem": {"bound": "smem_atomics", "achieved": smem_marks_rate,
                               "peak": peaks["smem_atomic_conflict_free"], "unit": "atomic ops/s",
                               "frac": smem_marks_rate / peaks["smem_atomic_conflict_free"],
@@ -347,8 +411,19 @@ def run_ours(args):
                      "plain_tests_per_s": world * BPSW_COUNT / (bpsw_plain_ms / 1e3),
                      "plain_ms_per_batch": bpsw_plain_ms, "batched_over_plain": bpsw_plain_ms / bpsw_ms,
                      "same_verdicts": bpsw_same, "primes": bpsw_primes,
+                     "roofline": imad_roofline((sprp_products + lucas_products) * IMAD_PER_PRODUCT_BPSW, bpsw_ms,
+                                               peaks["imad32"], {
+                         "products_base2_ladders": sprp_products, "products_lucas_ladders": lucas_products,
+                         "candidates_past_trial_division": bpsw_survivors, "lucas_candidates": bpsw_lucas_n,
+                         "imad_per_product": IMAD_PER_PRODUCT_BPSW,
+                         "note": "achieved = Montgomery products counted exactly from the inputs (base-2 ladders of "
+                                 "the trial-division survivors, Lucas ladders of the primes; chain squarings and "
+                                 "set-up left out: a lower bound) x 32-bit multiply instructions per product / "
+                                 "kernel time; peak = the 32-bit IMAD rate measured in this run"}),
                      "workload": "2^26 seeded odd u64 (60% uniform [2^40,2^64), 30% p*q near 2^62, "
                                  "10% (k+1)(2k+1) / Chernick), 4096 lists, log-uniform lengths"},
+            "config1": config1,
+            "reference_gpu": reference_gpu,
             "fermat": fermat,
             "chains": chains,
             "tuples": tuples,
@@ -369,7 +444,89 @@ def run_ours(args):
         print(json.dumps(line), flush=True)
 
 
-def run_fermat(e, world, rank, dev):
+C1_LO, C1_HI, C1_TILE_LOG2, C1_HASH_LOG2 = 10 ** 9, 11 * 10 ** 8, 18, 19
+
+
+def run_config1(e, dev, stream, flush, peaks, steps):
+    """Config 1: the plain segmented sieve of [1e9, 1.1e9) in 32 KiB segments (tiles of 2^18
+    bits), sieving primes up to isqrt of the sieved top, outputs pi, twins, the widest gap with
+    its start, 6-tuples and the FNV-1a hash of each 32 KiB segment's bitmap.  Device time with
+    CUDA events on the launching stream, L2 flushed between steps; the same call in the plain
+    form; marks per second of the dominant kernel against the shared-memory atomic rates."""
+    import ast
+    import ctypes as C
+    import torch
+    import mathpub_b200 as mp
+    L = mp.lib()
+    sp = stream.cuda_stream
+    nh = L.mp_sieve_nhashes(C1_LO, C1_HI, C1_HASH_LOG2)
+    d_out = torch.zeros(8, dtype=torch.int64, device=dev)
+    d_hash = torch.zeros(nh, dtype=torch.int64, device=dev)
+
+    def call(mode):
+        o = mp.SieveOpts(mode, C1_TILE_LOG2, 0, C1_HASH_LOG2, 0)
+        rc = L.mp_sieve_range_dev(e.handle, C1_LO, C1_HI, C.byref(o), C.c_void_p(d_out.data_ptr()), None,
+                                  C.c_void_p(d_hash.data_ptr()), None, C.c_void_p(sp))
+        if rc != 0:
+            raise mp.MathpubError(rc, L.mp_last_error(e.handle).decode())
+
+    def timed(mode, k):
+        for _ in range(3):
+            call(mode)
+        torch.cuda.synchronize()
+        tt = []
+        for _ in range(k):
+            flush.zero_()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            call(mode)
+            b.record(stream)
+            b.synchronize()
+            tt.append(a.elapsed_time(b))
+        return statistics.mean(tt)
+
+    ms = timed(mp.MODE_BATCHED, max(3, steps))
+    res = dict(zip(mp.STATS_FIELDS, [int(x) for x in d_out.cpu().numpy().view(np.uint64)]))
+    hashes = d_hash.cpu().numpy().view(np.uint64).copy()
+    plain_ms = timed(mp.MODE_PLAIN, 3)
+    plain_same = dict(zip(mp.STATS_FIELDS, [int(x) for x in d_out.cpu().numpy().view(np.uint64)])) == res and \
+        np.array_equal(d_hash.cpu().numpy().view(np.uint64), hashes)
+    e.profile(True)
+    call(mp.MODE_BATCHED)
+    torch.cuda.synchronize()
+    prof = e.profile_read()
+    e.profile(False)
+    kern_ms = prof["tile"][1] + prof.get("pipeline", (0, 0.0))[1]
+    primes = e.primes_range(3, int(np.sqrt(float(C1_HI + (1 << 16)))) + 2)
+    m_small, m_large = algorithmic_work(primes, C1_LO, C1_HI, 1 << C1_TILE_LOG2)
+    rate = (m_small + m_large) / (kern_ms / 1e3)
+    fix = None
+    try:
+        with open(os.path.join(ROOT, "tests", "golden", "configs.json")) as f:
+            c1 = json.load(f)["config1"]
+        want = ast.literal_eval(c1["stats"]) if isinstance(c1["stats"], str) else c1["stats"]
+        wh = ast.literal_eval(c1["hashes"]) if isinstance(c1["hashes"], str) else c1["hashes"]
+        fix = all(res[k] == want[k] for k in want) and [int(x) for x in hashes] == [int(x) for x in wh]
+    except Exception:
+        pass
+    span = C1_HI - C1_LO
+    return {"workload": "plain segmented sieve [1e9, 1.1e9), 32 KiB segments (2^18-bit tiles), sieving primes to "
+                        "isqrt(hi + tail); pi, twins, max gap + start, 6-tuples, per-32 KiB-segment FNV-1a hashes",
+            "value": span / (ms / 1e3), "unit": "ints/s", "ms_per_call": ms, "l2": "flushed between calls",
+            "plain": {"value": span / (plain_ms / 1e3), "ms_per_call": plain_ms, "batched_over_plain": plain_ms / ms,
+                      "same_results": plain_same},
+            "kernels_ms": {k: v[1] for k, v in prof.items() if v[0]},
+            "roofline_smem": {"bound": "smem_atomics", "achieved": rate, "unit": "atomic ops/s",
+                              "peak": peaks["smem_atomic_random"], "frac": rate / peaks["smem_atomic_random"],
+                              "peak_conflict_free": peaks["smem_atomic_conflict_free"],
+                              "marks": m_small + m_large, "kernel_ms": kern_ms,
+                              "note": "marks = wheel-30 multiples of the sieving primes >= 97 counted exactly; "
+                                      "peak = random-address shared atomicOr rate measured in this run"},
+            "results": res, "results_match_fixture": fix}
+
+
+def run_fermat(e, world, rank, dev, imad_peak):
     """Config 4: every prime in [1e12 + r 4e9, 1e12 + (r+1) 4e9) from the GPU sieve, base-2
     Fermat quotients with the full statistics; device time of the quotient and reduction
     kernels (events on the handle's stream), and the host-API call end to end."""
@@ -389,8 +546,15 @@ def run_fermat(e, world, rank, dev):
         fix = all(r[k] == c4[k] for k in ("primes", "tests", "near", "flt", "cks", "ordered_hash")) if lo == 10 ** 12 else None
     except Exception:
         pass
+    # products per prime: one per bit of p - 1 (square and double folded into one product where
+    # 8N < R) and the multiply that leaves Montgomery form; every p in the range has 40 bits
+    products = r["tests"] * (40 + 1)
+    roof = imad_roofline(products * IMAD_PER_PRODUCT_FERMAT_K3, kms, imad_peak, {
+        "products": products, "imad_per_product": IMAD_PER_PRODUCT_FERMAT_K3,
+        "note": "achieved = (bitlen(p - 1) + 1) three-limb Montgomery products per prime x 39 32-bit multiply "
+                "instructions per product / time of the quotient and statistics kernels"})
     return {"workload": "base-2 Fermat quotients of every prime in [1e12, 1e12+4e9) (per rank), 3-limb Montgomery",
-            "tests": r["tests"], "tests_per_s": r["tests"] / (kms / 1e3), "kernel_ms": kms,
+            "tests": r["tests"], "tests_per_s": r["tests"] / (kms / 1e3), "kernel_ms": kms, "roofline": roof,
             "e2e_tests_per_s": r["tests"] / wall, "e2e_ms": wall * 1e3, "near": r["near"], "flt": r["flt"],
             "cks": r["cks"], "results_match_fixture": fix,
             "job": {k: job[k] for k in ("primes", "tests", "near", "flt", "cks", "ordered_hash", "nhits")} if job else None}
@@ -540,6 +704,80 @@ def run_serving(e, args):
             "served_over_alone_throughput": (len(reqs) / span) / (len(sample) / (alone.sum() / 1e3))}
 
 
+REF_GPU_DIR = os.path.join(ROOT, "baseline", "_ref")
+
+
+def run_reference_gpu():
+    """The reference's own GPU programs, built unmodified from their sources for sm_100a into
+    baseline/_ref (oracle/Makefile, target refgpu), timed by their own clocks on this GPU:
+    a158939_cuda's sieve + gap scan over [1e15, 1e15+2e12), a350826_cuda's base-2 strong-test
+    benchmark on 2^24 odd numbers near 1e18, and wieferich_cuda's base-2 Fermat quotients of the
+    primes of [1e12, 1e12+4e9).  Each line is the program's own output."""
+    import re
+    progs = [
+        ("a158939_sieve_gap_scan", ["a158939_cuda", "bench", "1000000000000000", "-d", "2000000000000", "-N"],
+         r"bench: .*?: ([\d.]+) s, ([\d.e+]+) numbers/s", "numbers/s",
+         "the reference's GPU sieve + gap scan (A158939/cuda/a158939_cuda.cu) over [1e15, 1e15+2e12)"),
+        ("a350826_base2_sprp", ["a350826_cuda", "mrbench", "1000000000000000000", "16777216"],
+         r"grid \d+: ([\d.]+) s, ([\d.e+]+) tests/s", "tests/s",
+         "the reference's GPU base-2 strong probable-prime round (A350826/cuda/a350826_cuda.cu mrbench), 2^24 odd "
+         "numbers near 1e18; one round per number, not a full BPSW verdict"),
+        ("wieferich_base2", ["wieferich_cuda", "bench", "1000000000000", "-d", "4000000000", "-b", "2"],
+         r"bench .*? in ([\d.]+) s", "tests/s",
+         "the reference's GPU Fermat quotients (A001220/cuda/wieferich_cuda.cu), base 2, primes of [1e12, 1e12+4e9)"),
+    ]
+    out = {}
+    for name, cmd, pat, unit, what in progs:
+        exe = os.path.join(REF_GPU_DIR, cmd[0])
+        if not os.path.exists(exe):
+            out[name] = {"unavailable": f"{exe} not built (oracle/Makefile refgpu needs the reference tree)"}
+            continue
+        try:
+            t0 = time.perf_counter()
+            r = subprocess.run([exe] + cmd[1:], capture_output=True, text=True, timeout=180)
+            wall = time.perf_counter() - t0
+        except Exception as ex:
+            out[name] = {"unavailable": f"did not finish: {ex}"}
+            continue
+        text = r.stdout + r.stderr
+        rec = {"what": what, "rc": r.returncode, "wall_s": wall, "output": text.strip().splitlines()[-3:]}
+        ms = re.findall(pat, text)
+        if ms and name != "wieferich_base2":
+            best = max(float(m[1]) for m in ms)
+            rec.update({"value": best, "unit": unit, "seconds": float(ms[-1][0])})
+        elif ms:
+            tp = re.search(r"([\d.e+]+) tests/s", text)
+            if tp:
+                rec.update({"value": float(tp.group(1)), "unit": unit, "seconds": float(ms[-1])})
+        out[name] = rec
+    return out
+
+
+def imad_roofline(imad_ops, kernel_ms, peak, extra):
+    achieved = imad_ops / (kernel_ms / 1e3)
+    out = {"bound": "imad", "achieved": achieved, "peak": peak, "unit": "IMAD ops/s", "frac": achieved / peak,
+           "traffic": None, "peak_source": "measured in this run (mp_probe_peaks imad32)"}
+    out.update(extra)
+    return out
+
+
+def reference_twin_sieve(lo, hi, t):
+    """The reference's own CPU sieve for one output of this workload: A007508's twin-class bucket
+    sieve (count_twins_twin, A007508/a007508.c:514, built from its source into oracle/_ref) on the
+    same sample, rounded to multiples of 30.  It sieves 3 of every 15 odd residues (twin classes
+    only), so its integers/s is for the twin count alone."""
+    import oracle
+    if not oracle.have_ref_twins():
+        return None
+    a, b = -(-lo // 30) * 30, (hi // 30) * 30
+    t0 = time.perf_counter()
+    n = oracle.ref_twins(a, b, t)
+    dt = time.perf_counter() - t0
+    return {"value": (b - a) / dt, "unit": "ints/s", "cores": t, "kind": "reference", "twins": n,
+            "sample": f"twin pairs in [{a}, {b}) by A007508/a007508.c count_twins_twin, {t} threads, {dt:.3f} s "
+                      "(twin count only)"}
+
+
 def cpu_baseline(sample_log2=31):
     """The oracle's restatement of the reference's odd-only sieve (every output of the
     workload) on [1e15, 1e15 + 2^31) with all host threads."""
@@ -551,6 +789,9 @@ def cpu_baseline(sample_log2=31):
     dt = time.perf_counter() - t0
     out = {"value": (hi - lo) / dt, "unit": "ints/s", "cores": t, "kind": "port",
            "sample": f"[1e15, 1e15+2^{sample_log2}) with every output, {t} threads, {dt:.2f} s"}
+    tw = reference_twin_sieve(lo, hi, t)
+    if tw:
+        out["reference_twin_sieve"] = tw
     if oracle.have_ref():
         import mathpub_b200 as mp
         n, _ = mp.bpsw_workload(BPSW_SEED, 1 << 22, 0)
@@ -602,17 +843,22 @@ def run_reference(args):
         oracle.sieve_range(lo, lo + sample, block_log2=BLOCK_LOG2, hash_log2=HASH_LOG2, nthreads=t)
         times.append(time.perf_counter() - t0)
     value = sample * len(times) / sum(times)
+    tw = reference_twin_sieve(LO, LO + sample, t)
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "ints/s",
             "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "sample_per_step": "2^31 integers of the range, every output"},
             "cpu_baseline": {"value": value, "unit": "ints/s", "cores": t, "kind": "port",
-                             "sample": f"[1e15 + k 2^31, +2^31) per step, {t} threads; the reference's "
-                                       "primesieve-based range tools cannot be built here (primesieve is not "
-                                       "vendored), so the oracle's restatement of its odd-only sieve "
-                                       "(A228768/a228768.c:372-415) is timed"},
+                             "sample": f"[1e15 + k 2^31, +2^31) per step, {t} threads; the reference has no CPU "
+                                       "function that sieves a range with these outputs (its odd-only sieve in "
+                                       "A228768/a228768.c:372-415 runs an emirp test on every prime), so the "
+                                       "oracle's restatement of that sieve with every output is timed; the "
+                                       "reference's own twin-class sieve is timed beside it "
+                                       "(reference_twin_sieve)"},
             "e2e": {"value": value, "unit": "ints/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if tw:
+        line["reference_twin_sieve"] = tw
     print(json.dumps(line), flush=True)
 
 
