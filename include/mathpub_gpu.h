@@ -296,8 +296,9 @@ int mp_autotune(mp_handle *h, uint64_t lo, char *report, size_t cap);
  * mp_profile_enable(h, 1) brackets every launch of the timed kernels with CUDA events on the
  * stream it runs on (batched sieve calls then run directly instead of replaying a captured
  * graph); mp_profile_read fills, for the categories "scatter, tile, fold, hash, bpsw_batched,
- * bpsw_plain, fermat, fermat_stats" in that order, the launch counts and summed device
- * milliseconds since the previous read.
+ * bpsw_plain, fermat, fermat_stats, pipeline" in that order (the first ncat of them), the
+ * launch counts and summed device milliseconds since the previous read.  "pipeline" is the
+ * persistent launch that runs a batched sieve call's scatter and tile work together.
  * mp_probe_peaks measures device-wide rates (operations per second): shared-memory atomicOr
  * with the lanes of a warp on distinct banks and on random words, 32-bit integer
  * multiply-adds, and global atomicOr on random words of a 64 MB buffer (the L2 atomic rate).

@@ -352,7 +352,7 @@ class Engine:
         self._check(lib().mp_wieferich_range(self._h, lo, hi, C.byref(out)))
         return out.as_dict()
 
-    PROF_CATS = ["scatter", "tile", "fold", "hash", "bpsw_batched", "bpsw_plain", "fermat", "fermat_stats"]
+    PROF_CATS = ["scatter", "tile", "fold", "hash", "bpsw_batched", "bpsw_plain", "fermat", "fermat_stats", "pipeline"]
 
     def profile(self, on=True):
         self._check(lib().mp_profile_enable(self._h, 1 if on else 0))

@@ -169,6 +169,9 @@ struct Autotune {
     int sieve_threads = 0;
     int fermat_variant = 0;
     int bpsw_variant = 0;            // warps per CTA x candidates per chunk of the batched BPSW kernel
+    int scatter_staged = 0;          // 1: the staged (sorted) bucket scatter instead of the binned one
+    int bucket_div = 1;              // primes above tile bits / bucket_div (1, 2 or 4) go to the bucket scatter
+    int no_pipeline = 0;             // 1: batched sieve calls as a host loop of wave launches
     u64 tuned_at = 0;
 };
 
@@ -178,7 +181,7 @@ struct ChainDev;                     // the constellation sieve's plan and buffe
 // per-kernel timing for measurement: when enabled, each launch of a timed kernel category is
 // bracketed by CUDA events on its own stream; mp_profile_read sums them
 enum { PROF_SCATTER, PROF_TILE, PROF_FOLD, PROF_HASH, PROF_BPSW_BATCHED, PROF_BPSW_PLAIN, PROF_FERMAT,
-       PROF_FERMAT_STATS, PROF_NCAT };
+       PROF_FERMAT_STATS, PROF_PIPELINE, PROF_NCAT };
 struct ProfEv {
     int cat;
     cudaEvent_t a, b;

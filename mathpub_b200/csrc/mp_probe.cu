@@ -67,7 +67,7 @@ int mp_profile_enable(mp_handle *h, int on)
 }
 
 // per category: launches and summed milliseconds since the last read; names in order
-// "scatter tile fold hash bpsw_batched bpsw_plain fermat fermat_stats"
+// "scatter tile fold hash bpsw_batched bpsw_plain fermat fermat_stats pipeline"
 int mp_profile_read(mp_handle *h, uint64_t *launches, double *ms, int ncat)
 {
     if (!h || !launches || !ms) return MP_EINVAL;

@@ -64,7 +64,7 @@ struct TileArgs {
     const u32 *pat[MP_NPAT];
     u32 period[MP_NPAT];
     const u32 *rec;                      // bucket records of tiles [t0, t0 + nt) (nullable)
-    const u32 *reccnt;
+    u32 *reccnt;
     u32 reccap;
     TileSum *sums;                       // by global tile index
     u32 *bitmap32;                       // nullable
@@ -72,6 +72,14 @@ struct TileArgs {
     u64 *emit64;
     u32 *emit32;
     u32 *tstate;                         // per CTA: next multiple of each sparse thread-tier prime
+};
+
+// the per-launch (or per-item) part of a wave: its first tile and tile count, and its bucket
+// records and their counts; passed by value so that the argument structs stay in the
+// kernel's parameter space
+struct Wave {
+    u32 t0, wt;
+    u32 *rec, *cnt;
 };
 
 // state of a sparse thread-tier prime between the tiles of a CTA's run: (next bit relative to
@@ -160,6 +168,10 @@ __device__ __forceinline__ u32 bits_mask(u64 start, u64 bound)
     return n >= 32 ? 0xffffffffu : ((1u << n) - 1);
 }
 
+// a 16-byte bucket-record load: streaming through L1 in a kernel of its own, through L2 only
+// inside the pipeline kernel
+__device__ __forceinline__ uint4 rec_ld(const uint4 *p, bool l2_only) { return l2_only ? __ldcg(p) : __ldcs(p); }
+
 template <int TLOG>
 __device__ __forceinline__ void presieve(u32 *sm, const TileArgs &a, const u32 *s_off)
 {
@@ -195,14 +207,19 @@ __device__ __forceinline__ void presieve(u32 *sm, const TileArgs &a, const u32 *
     }
 }
 
-// EMIT = 0: statistics (+ optional bitmap); EMIT = 1: write the in-range primes
-template <int TLOG, int EMIT>
-__global__ void __launch_bounds__(1024) tile_kernel(TileArgs a)
+// Tiles [rb, re) of wave W (relative to W.t0), in order, by the whole CTA, with the tile in
+// shared memory `sm` (TW + HALO_WORDS words) and the carried state of the sparse thread-tier
+// primes in `tst`.  EMIT = 0: statistics (+ optional bitmap); EMIT = 1: write the in-range
+// primes.  PIPE: the tile runs inside the pipeline kernel, whose bucket records were written
+// by other CTAs of the same launch: they are read through L2 (not L1, which may hold the
+// lines of an earlier wave), and each tile's record count is reset once it is consumed, so
+// that the ring slot is clean for the wave after next.
+template <int TLOG, int EMIT, bool PIPE>
+__device__ __forceinline__ void tile_run(const TileArgs &a, const Wave W, u32 rb, u32 re, u32 *tst, u32 *sm)
 {
     constexpr u32 T = 1u << TLOG;
     constexpr u32 TW = T / 32;
     constexpr u32 NB = T + HALO_BITS;          // bits held in shared memory
-    extern __shared__ __align__(16) u32 sm[];  // TW + HALO_WORDS words
     __shared__ u32 s_off[MP_NPAT];
     __shared__ Part s_part[32];
     __shared__ u32 s_cnt[32];
@@ -210,16 +227,10 @@ __global__ void __launch_bounds__(1024) tile_kernel(TileArgs a)
     const u32 tid = threadIdx.x, nth = blockDim.x, lane = tid & 31, warp = tid >> 5, nwarps = nth >> 5;
     const u64 base = a.g.base, limit = a.g.limit, nbx = a.g.nbx;
 
-    // CTA b sieves the contiguous run of tiles [b per, (b + 1) per) of the launch, so that the
-    // sparse thread-tier primes carry their next multiple from one tile to the next
-    const u32 per = (a.nt + gridDim.x - 1) / gridDim.x;
-    u32 *const tst = a.tstate + (u64)blockIdx.x * (a.it1 - a.itd);
-    for (u32 run = 0; run < per; run++) {
-        const u32 rel = blockIdx.x * per + run;
-        if (rel >= a.nt) break;
-        const bool fresh = run == 0;                              // no carried state yet
-        const bool keep = run + 1 < per && rel + 1 < a.nt;        // the next tile follows here
-        const u32 t = a.t0 + rel;
+    for (u32 rel = rb; rel < re; rel++) {
+        const bool fresh = rel == rb;                             // no carried state yet
+        const bool keep = rel + 1 < re;                           // the next tile follows here
+        const u32 t = W.t0 + rel;
         const u64 G = (u64)t << TLOG;           // first bit of the tile
         const u64 x0 = base + 2 * G + 1;        // the odd number of that bit
         if (tid < MP_NPAT) s_off[tid] = (u32)((base / 2 + G) % a.period[tid]);
@@ -326,34 +337,35 @@ __global__ void __launch_bounds__(1024) tile_kernel(TileArgs a)
         // 4. large primes: bucket records of this tile.  Records and bitmap words are read or
         //    written once, with streaming cache hints, so that the prime table and the carried
         //    state of the sparse primes stay in L2.
-        if (a.rec) {
-            u32 n = __ldg(a.reccnt + rel);
+        if (W.rec) {
+            u32 n = PIPE ? __ldcg(W.cnt + rel) : __ldg(W.cnt + rel);
             if (n > a.reccap) n = a.reccap;
-            const u32 *R = a.rec + (u64)rel * a.reccap;       // reccap is a multiple of 4
+            const u32 *R = W.rec + (u64)rel * a.reccap;       // reccap is a multiple of 4
             const uint4 *R4 = (const uint4 *)R;
             const u32 n4 = n >> 2;
             u32 i = tid;
             for (; i + 3 * nth < n4; i += 4 * nth) {             // 16 records in flight per thread
-                const uint4 r0 = __ldcs(R4 + i), r1 = __ldcs(R4 + i + nth);
-                const uint4 r2 = __ldcs(R4 + i + 2 * nth), r3 = __ldcs(R4 + i + 3 * nth);
+                const uint4 r0 = rec_ld(R4 + i, PIPE), r1 = rec_ld(R4 + i + nth, PIPE);
+                const uint4 r2 = rec_ld(R4 + i + 2 * nth, PIPE), r3 = rec_ld(R4 + i + 3 * nth, PIPE);
                 const u32 js[16] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w,
                                     r2.x, r2.y, r2.z, r2.w, r3.x, r3.y, r3.z, r3.w};
 #pragma unroll
                 for (int k = 0; k < 16; k++) atomicOr(&sm[js[k] >> 5], 1u << (js[k] & 31));
             }
             for (; i < n4; i += nth) {
-                const uint4 r0 = __ldcs(R4 + i);
+                const uint4 r0 = rec_ld(R4 + i, PIPE);
                 atomicOr(&sm[r0.x >> 5], 1u << (r0.x & 31));
                 atomicOr(&sm[r0.y >> 5], 1u << (r0.y & 31));
                 atomicOr(&sm[r0.z >> 5], 1u << (r0.z & 31));
                 atomicOr(&sm[r0.w >> 5], 1u << (r0.w & 31));
             }
             for (u32 k = (n4 << 2) + tid; k < n; k += nth) {
-                const u32 j = __ldcs(R + k);
+                const u32 j = PIPE ? __ldcg(R + k) : __ldcs(R + k);
                 atomicOr(&sm[j >> 5], 1u << (j & 31));
             }
         }
         __syncthreads();
+        if (PIPE && W.rec && tid == 0) W.cnt[rel] = 0;            // every thread has read it
 
         // 5. scans
         if (!EMIT) {
@@ -552,6 +564,19 @@ __global__ void __launch_bounds__(1024) tile_kernel(TileArgs a)
         }
         __syncthreads();
     }
+}
+
+// CTA b sieves the contiguous run of tiles [b per, (b + 1) per) of the launch, so that the
+// sparse thread-tier primes carry their next multiple from one tile to the next
+template <int TLOG, int EMIT>
+__global__ void __launch_bounds__(1024) tile_kernel(TileArgs a)
+{
+    extern __shared__ __align__(16) u32 sm[];  // TW + HALO_WORDS words
+    const u32 per = (a.nt + gridDim.x - 1) / gridDim.x;
+    const u32 rb = blockIdx.x * per;
+    const u32 re = min(rb + per, a.nt);
+    const Wave W = {a.t0, a.nt, (u32 *)a.rec, a.reccnt};
+    if (rb < re) tile_run<TLOG, EMIT, false>(a, W, rb, re, a.tstate + (u64)blockIdx.x * (a.it1 - a.itd), sm);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -754,6 +779,227 @@ __global__ void __launch_bounds__(SC_THREADS, SC_CTAS_PER_SM) scatter_kernel(Sca
         }
     }
     scatter_flush(a, stage, sorted, hist, gb, &s_fill, s_wsum);
+}
+
+// The binned form of the same scatter (the default): one CTA of SB_THREADS threads per SM,
+// whose shared memory holds a bin of `binc` records per tile of the wave.  A record goes
+// straight into its tile's bin (one shared atomic for the slot), so no sort is needed: every
+// SB_FLUSH_ROUNDS rounds (the same round in every thread, so the decision is uniform) each
+// warp writes whole bins of its tiles as coalesced runs, with one global atomic per tile to
+// reserve the run in the bucket.  A record that finds its bin full goes to an overflow list,
+// and past that straight to its bucket with a global atomic of its own; results are exact
+// either way.
+#define SB_THREADS 1024
+#define SB_OVF 1024
+#define SB_FLUSH_ROUNDS 4
+
+__device__ __forceinline__ void sb_direct(const ScatterArgs &a, const Wave &W, u32 tl, u32 off)
+{
+    const u32 slot = atomicAdd(W.cnt + tl, 1u);
+    if (slot < a.cap) __stcs(W.rec + (u64)tl * a.cap + slot, off);
+    else atomicOr(a.err, 2u);
+}
+
+__device__ __forceinline__ void sb_flush(const ScatterArgs &a, const Wave &W, const u32 *bin, u32 *cnt, const u32 *ovf,
+                                         u32 *s_novf, u32 binc)
+{
+    const u32 tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5, wt = W.wt;
+    // warp w: tiles w * 32 + l for its lanes l, then every 32 * nwarps; lane l reserves the
+    // run of tile l of the group, then the warp writes the group's runs one after the other
+    for (u32 t0 = warp * 32; t0 < wt; t0 += 32 * nwarps) {
+        const u32 t = t0 + lane;
+        const u32 n = t < wt ? min(cnt[t], binc) : 0u;
+        u32 g = 0;
+        if (n) {
+            g = atomicAdd(W.cnt + t, n);
+            if (g + n > a.cap) atomicOr(a.err, 2u);
+        }
+        u32 m = __ballot_sync(0xffffffffu, n != 0);
+        while (m) {
+            const u32 l = __ffs(m) - 1;
+            m &= m - 1;
+            const u32 nl = __shfl_sync(0xffffffffu, n, l), gl = __shfl_sync(0xffffffffu, g, l);
+            const u32 *b = bin + (t0 + l) * binc;
+            u32 *dst = W.rec + (u64)(t0 + l) * a.cap;
+            for (u32 i = lane; i < nl; i += 32)
+                if (gl + i < a.cap) __stcs(dst + gl + i, b[i]);
+        }
+    }
+    const u32 no = min(*s_novf, (u32)SB_OVF);
+    for (u32 i = tid; i < no; i += blockDim.x)
+        sb_direct(a, W, ovf[i] >> SC_OFF_BITS, ovf[i] & ((1u << SC_OFF_BITS) - 1u));
+    __syncthreads();
+    for (u32 t = tid; t < wt; t += blockDim.x) cnt[t] = 0;
+    if (tid == 0) *s_novf = 0;
+    __syncthreads();
+}
+
+// the large primes [k_begin, k_end) of the table over wave W, by the whole CTA, with the bins
+// in shared memory `ssm` (W.wt * binc + W.wt + SB_OVF words)
+__device__ __forceinline__ void scatter_binned_run(const ScatterArgs &a, const Wave W, u32 k_begin, u32 k_end, u32 binc,
+                                                   u32 *ssm)
+{
+    const u32 wt = W.wt;
+    u32 *bin = ssm, *cnt = ssm + wt * binc, *ovf = cnt + wt;
+    __shared__ u32 s_novf;
+    const u32 tid = threadIdx.x, nth = blockDim.x, tlog = a.tlog, tmask = (1u << tlog) - 1;
+    for (u32 i = tid; i < wt; i += nth) cnt[i] = 0;
+    if (tid == 0) s_novf = 0;
+    const u64 wstart = (u64)W.t0 << tlog;
+    u64 wend = (u64)(W.t0 + wt) << tlog;
+    if (wend > a.nbx) wend = a.nbx;
+    u64 wend_halo = wend + HALO_BITS;
+    if (wend_halo > a.nbx) wend_halo = a.nbx;
+    const u64 x0 = a.base + 2 * wstart + 1;
+    const u32 xm = (u32)(x0 % 30u);
+    const u32 span = (u32)(wend_halo - wstart);          // < 2^31 (checked by the planner)
+    u32 k = k_begin + tid;
+    u32 jj[8], turn = 0;
+    bool have = false;
+    __syncthreads();
+    for (u32 round = 1;; round++) {
+        while (!have && k < k_end) {
+            have = scatter_setup(a, k, x0, xm, span, jj, turn);
+            k += nth;
+        }
+        if (have) {
+            // one turn of the wheel: up to 8 records, each into its tile's bin
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+                const u32 j = jj[i];
+                if (j < span) {
+                    const u32 tl = j >> tlog, off = j & tmask;
+                    if (tl < wt) {
+                        const u32 slot = atomicAdd(&cnt[tl], 1u);
+                        if (slot < binc) bin[tl * binc + slot] = off;
+                        else {
+                            const u32 o = atomicAdd(&s_novf, 1u);
+                            if (o < SB_OVF) ovf[o] = (tl << SC_OFF_BITS) | off;
+                            else sb_direct(a, W, tl, off);
+                        }
+                    }
+                    if (off < HALO_BITS && tl >= 1 && tl - 1 < wt) sb_direct(a, W, tl - 1, off + (1u << tlog));
+                    jj[i] = j + turn;
+                }
+            }
+            have = jj[0] < span;
+        }
+        const int more = __syncthreads_or(have);            // every append of the round is done
+        if (!more) break;
+        if (round % SB_FLUSH_ROUNDS == 0) sb_flush(a, W, bin, cnt, ovf, &s_novf, binc);
+    }
+    sb_flush(a, W, bin, cnt, ovf, &s_novf, binc);
+}
+
+__global__ void __launch_bounds__(SB_THREADS, 1) scatter_binned_kernel(ScatterArgs a, u32 binc)
+{
+    extern __shared__ __align__(16) u32 ssm[];
+    const Wave W = {a.t0, a.wt, a.rec, a.cnt};
+    scatter_binned_run(a, W, __ldg(a.bounds + blockIdx.x), __ldg(a.bounds + blockIdx.x + 1), binc, ssm);
+}
+
+// ---------------------------------------------------------------------------------------
+// the pipeline: every wave of a range in one persistent launch
+//
+// Work items, numbered in the order the device queue hands them out:
+//   S(0) ... S(1) T(0) ... S(2) T(1) ... S(W-1) T(W-2) ... T(W-1)
+// S(w, r) is the binned scatter of the large primes [bounds[r], bounds[r+1]) over wave w;
+// T(w, r) sieves tiles [r run, (r+1) run) of wave w.  The records of wave w live in ring slot
+// w & 1.  T(w, .) waits until every S(w, .) has finished; S(w, .) for w >= 2 waits until
+// every T(w-2, .) has finished with the slot (each tile item resets the record counts it has
+// consumed, so the slot is clean).  A CTA only ever waits for items that the queue handed out
+// before its own, to CTAs that are running them, so the waits always end; each is still
+// bounded, and on running out it sets bit 8 of the error flag (the call then fails).
+// Scatter items of the next wave run beside the tile items of this one on other SMs, and no
+// kernel boundary separates the waves.
+// ---------------------------------------------------------------------------------------
+
+struct PipeArgs {
+    TileArgs ta;                 // geometry, tiers, patterns and outputs
+    ScatterArgs sa;              // scatter parameters
+    u32 nwaves, wt, ntiles;      // waves of wt tiles, the last one holding the rest of ntiles
+    u32 nscat, run, binc;        // scatter items per wave, tiles per tile item, records per bin
+    u32 *rec[2], *cnt[2];        // the record ring
+    u32 *ctl;                    // [0] next item, [1 + w] S(w) done, [1 + nwaves + w] T(w) done
+    u32 spin_limit;              // polls of a wait before it gives up
+};
+
+__device__ __forceinline__ u32 pipe_wave_tiles(const PipeArgs &p, u32 w)
+{
+    return w + 1 < p.nwaves ? p.wt : p.ntiles - w * p.wt;
+}
+__device__ __forceinline__ u32 pipe_titems(const PipeArgs &p, u32 w) { return (pipe_wave_tiles(p, w) + p.run - 1) / p.run; }
+
+__device__ __forceinline__ u32 pipe_total(const PipeArgs &p)
+{
+    const u32 tf = (p.wt + p.run - 1) / p.run;
+    return p.nscat + (p.nwaves - 1) * (p.nscat + tf) + pipe_titems(p, p.nwaves - 1);
+}
+
+// item i -> kind (0 scatter, 1 tiles), wave, index within the wave's items of that kind
+__device__ __forceinline__ void pipe_decode(const PipeArgs &p, u32 i, u32 &kind, u32 &w, u32 &r)
+{
+    if (i < p.nscat) { kind = 0; w = 0; r = i; return; }
+    const u32 tf = (p.wt + p.run - 1) / p.run, B = p.nscat + tf, j = i - p.nscat, b = j / B;
+    if (b < p.nwaves - 1) {
+        const u32 q = j - b * B;
+        if (q < p.nscat) { kind = 0; w = b + 1; r = q; }
+        else { kind = 1; w = b; r = q - p.nscat; }
+    } else {
+        kind = 1; w = p.nwaves - 1; r = j - (p.nwaves - 1) * B;
+    }
+}
+
+// thread 0 polls *flag until it reaches need (bounded), then the CTA goes on together
+__device__ __forceinline__ void pipe_wait(const PipeArgs &p, const u32 *flag, u32 need)
+{
+    if (threadIdx.x == 0) {
+        u32 polls = 0;
+        while (*(volatile const u32 *)flag < need) {
+            if (++polls > p.spin_limit) { atomicOr(p.sa.err, 8u); break; }
+            __nanosleep(256);
+        }
+        __threadfence();
+    }
+    __syncthreads();
+}
+
+// every thread's writes of the item are made visible, then thread 0 counts the item done
+__device__ __forceinline__ void pipe_signal(u32 *flag)
+{
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) atomicAdd(flag, 1u);
+}
+
+template <int TLOG>
+__global__ void __launch_bounds__(1024, 1) sieve_pipeline_kernel(PipeArgs p)
+{
+    extern __shared__ __align__(16) u32 dyn[];
+    __shared__ u32 s_item;
+    const u32 total = pipe_total(p);
+    u32 *const sdone = p.ctl + 1, *const tdone = p.ctl + 1 + p.nwaves;
+    u32 *const tst = p.ta.tstate + (u64)blockIdx.x * (p.ta.it1 - p.ta.itd);
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(p.ctl, 1u);
+        __syncthreads();
+        const u32 it = s_item;
+        __syncthreads();                                   // s_item is read before it is reused
+        if (it >= total) break;
+        u32 kind, w, r;
+        pipe_decode(p, it, kind, w, r);
+        const Wave W = {w * p.wt, pipe_wave_tiles(p, w), p.rec[w & 1], p.cnt[w & 1]};
+        if (kind == 0) {
+            if (w >= 2) pipe_wait(p, tdone + (w - 2), pipe_titems(p, w - 2));
+            scatter_binned_run(p.sa, W, __ldg(p.sa.bounds + r), __ldg(p.sa.bounds + r + 1), p.binc, dyn);
+            pipe_signal(sdone + w);
+        } else {
+            pipe_wait(p, sdone + w, p.nscat);
+            const u32 rb = r * p.run, re = min(rb + p.run, W.wt);
+            tile_run<TLOG, 0, true>(p.ta, W, rb, re, tst, dyn);
+            pipe_signal(tdone + w);
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------------------
@@ -1077,14 +1323,16 @@ int mp_patterns_ensure(mp_handle *h)
 
 struct Tiers { u32 iw0, iw1, itd, it1, iend; };
 
-static Tiers tiers_for(const PrimeTable &tb, u32 tlog, u64 top)
+// qbucket: the primes above it go to the bucket scatter (the tile size, or a half or quarter
+// of it when the autotuner finds that moving the sparsest thread-tier primes to buckets pays)
+static Tiers tiers_for(const PrimeTable &tb, u32 tlog, u64 top, u64 qbucket)
 {
     Tiers r;
     const u64 sq = mp_isqrt64(top - 1) + 1;
     r.iend = (u32)tb.count_le(sq);
     r.iw0 = (u32)std::min<u64>(tb.count_le(PAT_MAXQ), r.iend);
     r.iw1 = (u32)std::min<u64>(tb.count_le(QWARP - 1), r.iend);
-    r.it1 = (u32)std::min<u64>(tb.count_le(1ull << tlog), r.iend);
+    r.it1 = (u32)std::min<u64>(tb.count_le(qbucket), r.iend);
     r.itd = std::max(r.iw1, (u32)std::min<u64>(tb.count_le((1ull << tlog) / 32 - 1), r.it1));
     return r;
 }
@@ -1133,10 +1381,10 @@ static int tile_ctas_per_sm(u32 tlog, int nth)
 // expected bucket records per tile for the large primes (Mertens' theorem: the sum of 1/q
 // over primes in (a, b] is about ln(ln b / ln a); the wheel of 30 keeps 8 of every 15 odd
 // multiples), with a margin
-static u32 bucket_cap(u32 tlog, u64 qmax)
+static u32 bucket_cap(u32 tlog, u64 qlo, u64 qmax)
 {
     const double T = (double)(1u << tlog) + HALO_BITS;
-    const double a = (double)(1u << tlog);
+    const double a = (double)qlo;
     double s = qmax > (u64)a ? log(log((double)qmax) / log(a)) * (8.0 / 15.0) : 0.0;
     double e = T * s * 1.06 + 8.0 * sqrt(T * s + 1.0) + 4096.0;
     if (e > 4.0e9) e = 4.0e9;
@@ -1161,13 +1409,15 @@ static int plan_sieve(mp_handle *h, const PrimeTable &tb, u64 lo, u64 hi, u32 tl
     const u64 ntiles = (P.g.nbx + (1ull << tlog) - 1) >> tlog;
     if (ntiles >= (1ull << 31)) return mp_set_error(h, MP_ERANGE, "range too long (%llu tiles)", (unsigned long long)ntiles);
     P.g.ntiles = (u32)ntiles;
-    P.ti = tiers_for(tb, tlog, top);
+    const u32 bdiv = h->tune.bucket_div == 2 || h->tune.bucket_div == 4 ? (u32)h->tune.bucket_div : 1u;
+    const u64 qbucket = (1ull << tlog) / bdiv;
+    P.ti = tiers_for(tb, tlog, top, qbucket);
     if (tb.limit < mp_isqrt64(top - 1)) return mp_set_error(h, MP_EINVAL, "prime table too small");
     P.nth = nth;
     P.large = P.ti.iend > P.ti.it1;
     if (P.large) {
         const u64 qmax = tb.host[P.ti.iend - 1];
-        P.cap = bucket_cap(tlog, qmax);
+        P.cap = bucket_cap(tlog, qbucket, qmax);
         // wave: enough tiles to keep every SM busy for several tiles (8 per SM), within
         // 2 GB of records
         u64 wt = 8ull * (u64)h->sm_count;
@@ -1213,14 +1463,41 @@ static cudaError_t launch_scatter(const ScatterArgs &s, u32 nblk, cudaStream_t s
     return cudaGetLastError();
 }
 
+// records per tile bin of the binned scatter for a wave of wt tiles in `smem_max` bytes of
+// shared memory; 0 when the bins would be too small to be worth it
+static u32 binned_capacity(u32 wt, int smem_max)
+{
+    const long long room = (long long)smem_max - 4ll * (wt + SB_OVF) - 256;
+    if (room <= 0) return 0;
+    u64 c = (u64)room / (4ull * wt);
+    if (c > 96) c = 96;
+    return c >= 8 ? (u32)c : 0u;
+}
+
+static cudaError_t launch_scatter_binned(const ScatterArgs &s, u32 nblk, u32 binc, int smem_max, cudaStream_t st)
+{
+    const size_t smem = ((size_t)s.wt * binc + s.wt + SB_OVF) * 4;
+    static bool attr_set[16] = {false};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 16) return cudaErrorInvalidDevice;
+    if (!attr_set[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(scatter_binned_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+        if (e != cudaSuccess) return e;
+        attr_set[dev] = true;
+    }
+    scatter_binned_kernel<<<nblk, SB_THREADS, smem, st>>>(s, binc);
+    return cudaGetLastError();
+}
+
 // CTA boundaries for the scatter kernel: contiguous runs of the large primes [i0, i1) of equal
 // work, where a prime's work is its expected hits in a wave (proportional to 1/q) plus its
 // set-up, worth about 8 hits in a wave of 2^30 bits.  SC_CTAS_PER_SM persistent CTAs per SM.  Built on
 // the host from the table's prefix sums of 1/q and uploaded once per prime range (never
 // inside a capture).
-static int scatter_bounds(mp_handle *h, const PrimeTable &tb, u32 i0, u32 i1, cudaStream_t st)
+static int scatter_bounds(mp_handle *h, const PrimeTable &tb, u32 i0, u32 i1, u32 per_sm, cudaStream_t st)
 {
-    const u32 want = (u32)std::max<u64>(1, std::min<u64>((u64)h->sm_count * SC_CTAS_PER_SM, i1 - i0));
+    const u32 want = (u32)std::max<u64>(1, std::min<u64>((u64)h->sm_count * per_sm, i1 - i0));
     if (h->scat_key[0] == i0 && h->scat_key[1] == i1 && h->scat_key[2] == want && h->scat_nblk) return MP_OK;
     if (tb.inv_prefix.size() < (size_t)i1 + 1) return mp_set_error(h, MP_EINVAL, "prime table has no prefix sums");
     const double c = 8.0 / ((double)(1u << 30) * 8.0 / 15.0);      // set-up, in units of 1/q
@@ -1248,6 +1525,80 @@ static int scatter_bounds(mp_handle *h, const PrimeTable &tb, u32 i0, u32 i1, cu
     return MP_OK;
 }
 
+template <int TLOG>
+static cudaError_t launch_pipeline(const PipeArgs &p, int grid, int nth, size_t smem, int smem_max, cudaStream_t st)
+{
+    static bool attr_set[16] = {false};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 16) return cudaErrorInvalidDevice;
+    if (!attr_set[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(sieve_pipeline_kernel<TLOG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             smem_max);
+        if (e != cudaSuccess) return e;
+        attr_set[dev] = true;
+    }
+    sieve_pipeline_kernel<TLOG><<<grid, nth, smem, st>>>(p);
+    return cudaGetLastError();
+}
+
+template <int TLOG>
+static cudaError_t pipeline_ctas_per_sm(int nth, size_t smem, int *per_sm)
+{
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, sieve_pipeline_kernel<TLOG>, nth, smem);
+}
+
+// the batched form in one persistent launch (sieve_pipeline_kernel): every wave's scatter and
+// tile items from one device queue, the records in a ring of two wave slots
+static int run_pipeline(mp_handle *h, const PrimeTable &tb, const SievePlan &P, TileArgs a, u32 binc, int smem_max,
+                        int grid_pers, cudaStream_t st)
+{
+    const int nth = P.nth;
+    const u32 tlog = P.g.tlog, nw = P.nwaves;
+    const size_t tile_smem = ((1u << tlog) / 32 + HALO_WORDS) * 4;
+    const size_t scat_smem = ((size_t)P.wt * binc + P.wt + SB_OVF) * 4;
+    const size_t smem = std::max(tile_smem, scat_smem);
+    int per_sm = 0;
+    cudaError_t e = tlog == 18 ? pipeline_ctas_per_sm<18>(nth, smem, &per_sm)
+                  : tlog == 19 ? pipeline_ctas_per_sm<19>(nth, smem, &per_sm)
+                               : pipeline_ctas_per_sm<20>(nth, smem, &per_sm);
+    MP_CUDA(h, e);
+    if (per_sm < 1) return mp_set_error(h, MP_EINVAL, "the pipeline kernel does not fit on an SM");
+    const int grid = h->sm_count * per_sm;
+    // carried state: one slot per sparse prime per CTA of whichever launch is larger
+    MP_CUDA(h, h->tstate.ensure((size_t)std::max(grid, grid_pers) * (P.ti.it1 - P.ti.itd) * 4 + 64));
+    a.tstate = h->tstate.as<u32>();
+    MP_CUDA(h, h->rec.ensure((size_t)2 * P.wt * P.cap * 4));
+    MP_CUDA(h, h->reccnt.ensure(((size_t)2 * P.wt + 1 + 2 * (size_t)nw) * 4 + 64));
+    u32 *cnt0 = h->reccnt.as<u32>();
+    MP_CUDA(h, cudaMemsetAsync(cnt0, 0, ((size_t)2 * P.wt + 1 + 2 * (size_t)nw) * 4, st));
+    PipeArgs p;
+    memset(&p, 0, sizeof p);
+    p.ta = a;
+    p.ta.reccap = P.cap;
+    ScatterArgs &s = p.sa;
+    s.base = P.g.base; s.tlog = tlog; s.nbx = P.g.nbx;
+    s.q = tb.q.as<u32>(); s.magic = tb.magic.as<u64>();
+    s.bounds = h->scat_bounds.as<u32>();
+    s.cap = P.cap; s.err = h->errflag.as<u32>();
+    p.nwaves = nw; p.wt = P.wt; p.ntiles = P.g.ntiles;
+    p.nscat = h->scat_nblk;
+    p.run = std::max<u32>(1, P.wt / (u32)grid);
+    p.binc = binc;
+    p.rec[0] = h->rec.as<u32>();
+    p.rec[1] = p.rec[0] + (size_t)P.wt * P.cap;
+    p.cnt[0] = cnt0;
+    p.cnt[1] = cnt0 + P.wt;
+    p.ctl = cnt0 + 2 * P.wt;
+    p.spin_limit = 1u << 23;
+    ProfScope ps(h, PROF_PIPELINE, st);
+    e = tlog == 18 ? launch_pipeline<18>(p, grid, nth, smem, smem_max, st)
+      : tlog == 19 ? launch_pipeline<19>(p, grid, nth, smem, smem_max, st)
+                   : launch_pipeline<20>(p, grid, nth, smem, smem_max, st);
+    MP_CUDA(h, e);
+    return MP_OK;
+}
+
 // mode: 0 batched (waves of tile launches, each CTA a contiguous run of tiles), 1 plain (the
 // reference's per-segment launch loop on a full grid: one launch per group of sm_count
 // segments, one segment per CTA, each set up from scratch, with its own bucket scatter)
@@ -1268,7 +1619,14 @@ static int run_tiles(mp_handle *h, const PrimeTable &tb, const SievePlan &P, Til
         MP_CUDA(h, h->rec.ensure((size_t)wmax * P.cap * 4));
         MP_CUDA(h, h->reccnt.ensure((size_t)wmax * 4 * 2));
     }
-    if (P.large) MP_TRY(scatter_bounds(h, tb, P.ti.it1, P.ti.iend, st));
+    // the binned scatter (one CTA per SM) unless the wave's bins would not fit or the handle
+    // asks for the staged form
+    int smem_max = 0;
+    MP_CUDA(h, cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
+    smem_max -= 1024;                                   // the kernel's static shared memory and slack
+    const u32 binc = P.large && h->tune.scatter_staged == 0 ? binned_capacity(wmax, smem_max) : 0u;
+    if (P.large) MP_TRY(scatter_bounds(h, tb, P.ti.it1, P.ti.iend, binc ? 1u : (u32)SC_CTAS_PER_SM, st));
+    if (mode == 0 && !emit && binc && !h->tune.no_pipeline) return run_pipeline(h, tb, P, a, binc, smem_max, grid_pers, st);
     for (u32 L = 0; L < nlaunch; L++) {
         const u32 t0 = L * wmax;
         const u32 nt = std::min(wmax, P.g.ntiles - t0);
@@ -1282,7 +1640,8 @@ static int run_tiles(mp_handle *h, const PrimeTable &tb, const SievePlan &P, Til
             const u32 nblk = h->scat_nblk;
             {
                 ProfScope ps(h, PROF_SCATTER, st);
-                MP_CUDA(h, launch_scatter(s, nblk, st));
+                if (binc) MP_CUDA(h, launch_scatter_binned(s, nblk, binc, smem_max, st));
+                else MP_CUDA(h, launch_scatter(s, nblk, st));
             }
             a.rec = s.rec; a.reccnt = s.cnt; a.reccap = P.cap;
         }
@@ -1303,6 +1662,7 @@ static int check_errflag(mp_handle *h, cudaStream_t st)
         MP_CUDA(h, cudaMemsetAsync(h->errflag.p, 0, 4, st));
         if (e & 2) return mp_set_error(h, MP_EOVERFLOW, "bucket records exceeded their capacity");
         if (e & 4) return mp_set_error(h, MP_ERANGE, "no prime follows the last prime of the range within the tail");
+        if (e & 8) return mp_set_error(h, MP_ETIMEOUT, "a wait of the sieve pipeline ran out (its results are not valid)");
         return mp_set_error(h, MP_ETIMEOUT, "device error flag 0x%x", e);
     }
     return MP_OK;

@@ -1,6 +1,8 @@
 // mp_tune.cu -- the measured autotuner: times the sieve tile geometry (bits per tile x
-// threads per CTA) and the Fermat kernel variants (limbs fixed by p, one or two primes per
-// thread) on the device with CUDA events, and keeps the fastest per handle.  The reference
+// threads per CTA), the bucket scatter's form, the bucket threshold, the batched form
+// (persistent pipeline or wave loop), the Fermat kernel variants (limbs fixed by p, one or two
+// primes per thread) and the batched BPSW kernel's warps per CTA x candidates per queue chunk
+// on the device with CUDA events, and keeps the fastest per handle.  The reference
 // chooses its wheel and chunk by a fitted cost model (auto_wheel / auto_chunk,
 // A350826/a350826.c:1976-2015); here the candidates are timed instead.
 #include "mp_common.cuh"
@@ -50,7 +52,35 @@ extern "C" int mp_autotune(mp_handle *h, uint64_t lo, char *report, size_t cap)
     h->tune.sieve_tile_log2 = (int)bt;
     h->tune.sieve_threads = (int)bn;
     h->tune.tuned_at = lo;
-    snprintf(line, sizeof line, "sieve choice: tile 2^%u, %u threads\n", bt, bn);
+    // one knob at a time at that geometry, each against a 2^32-integer range:
+    //   the bucket scatter's form: binned (one CTA per SM, a bin per tile) or staged (three
+    //   CTAs per SM, a sorted stage);
+    //   the bucket threshold: primes above the tile size, half of it or a quarter of it go to
+    //   the scatter (fewer visits of sparse primes per tile against more bucket records);
+    //   the batched form as one persistent pipeline launch or as a host loop of wave launches
+    struct Knob { const char *name; int *field; int vals[3]; int nv; const char *labels[3]; };
+    Knob knobs[3] = {
+        {"scatter", &h->tune.scatter_staged, {0, 1, 0}, 2, {"binned", "staged", ""}},
+        {"bucket threshold", &h->tune.bucket_div, {1, 2, 4}, 3, {"tile", "tile/2", "tile/4"}},
+        {"batched form", &h->tune.no_pipeline, {0, 1, 0}, 2, {"pipeline", "wave loop", ""}},
+    };
+    for (Knob &k : knobs) {
+        float kb = 1e30f;
+        int kv = k.vals[0];
+        for (int i = 0; i < k.nv; i++) {
+            *k.field = k.vals[i];
+            float ms = 0;
+            const int r = time_sieve(h, lo, lo + span, bt, bn, d_out, &ms);
+            if (r != MP_OK) { *k.field = k.vals[0]; return r; }
+            snprintf(line, sizeof line, "%s %s: %.3f ms / 2^32\n", k.name, k.labels[i], ms / 3);
+            rep += line;
+            if (ms < kb) { kb = ms; kv = k.vals[i]; }
+        }
+        *k.field = kv;
+    }
+    snprintf(line, sizeof line, "sieve choice: tile 2^%u, %u threads, %s scatter, bucket threshold tile/%d, %s\n", bt,
+             bn, h->tune.scatter_staged ? "staged" : "binned", h->tune.bucket_div,
+             h->tune.no_pipeline ? "wave loop" : "pipeline");
     rep += line;
     // Fermat: 2^20 primes near max(lo, 1e12), one vs two per thread
     u64 plo = std::max<u64>(lo, 1000000000000ull);
@@ -79,6 +109,44 @@ extern "C" int mp_autotune(mp_handle *h, uint64_t lo, char *report, size_t cap)
         if (ms < fb) { fb = ms; fv = v; }
     }
     h->tune.fermat_variant = fv & 2;
+    // batched BPSW: 2^20 seeded odd candidates (three in four in [2^62, 2^64), the rest in
+    // [2^40, 2^62)), one list, each warps x chunk pair the kernel is built for
+    {
+        const u64 cnt = 1ull << 20;
+        std::vector<u64> cand(cnt);
+        u64 z = 0x5eed5eedull;
+        for (u64 i = 0; i < cnt; i++) {
+            z += MP_GOLD;
+            u64 x = mp_mix64(z);
+            x = (i & 3) ? (x | (1ull << 62)) : ((x >> 24) | (1ull << 40));
+            cand[i] = x | 1;
+        }
+        MP_CUDA(h, h->bpsw_n.ensure(cnt * 8));
+        MP_CUDA(h, h->bpsw_bits.ensure(cnt / 8 + 64));
+        MP_CUDA(h, cudaMemcpyAsync(h->bpsw_n.p, cand.data(), cnt * 8, cudaMemcpyHostToDevice, h->stream));
+        const u64 offs[2] = {0, cnt};
+        const u32 lens[1] = {(u32)cnt};
+        float bb = 1e30f;
+        int bv = 0;
+        for (int v = 0; v < 4; v++) {
+            h->tune.bpsw_variant = v;
+            MP_TRY(mp_bpsw_run(h, h->bpsw_n.as<u64>(), offs, lens, 1, h->bpsw_bits.as<u32>(), MP_MODE_BATCHED, h->stream));
+            MP_CUDA(h, cudaEventRecord(h->ev0, h->stream));
+            for (int r = 0; r < 3; r++)
+                MP_TRY(mp_bpsw_run(h, h->bpsw_n.as<u64>(), offs, lens, 1, h->bpsw_bits.as<u32>(), MP_MODE_BATCHED,
+                                   h->stream));
+            MP_CUDA(h, cudaEventRecord(h->ev1, h->stream));
+            MP_CUDA(h, cudaEventSynchronize(h->ev1));
+            float ms = 0;
+            MP_CUDA(h, cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+            snprintf(line, sizeof line, "bpsw %s: %.3f ms for 2^20 candidates\n", mp_bpsw_variant_name(v), ms / 3);
+            rep += line;
+            if (ms < bb) { bb = ms; bv = v; }
+        }
+        h->tune.bpsw_variant = bv;
+        snprintf(line, sizeof line, "bpsw choice: %s\n", mp_bpsw_variant_name(bv));
+        rep += line;
+    }
     if (report && cap) {
         strncpy(report, rep.c_str(), cap - 1);
         report[cap - 1] = 0;
