@@ -11,10 +11,10 @@
 // Two launch structures:
 //   plain    one launch per candidate list, one thread per candidate, all phases inline;
 //   batched  one persistent launch over every list: warps pop chunks of candidates from a
-//            device work queue, trial-divide them, and file the survivors in two classes by
-//            size: below 2^62 (from the front of a shared-memory list; these run the lazy
-//            Montgomery products) and above (from the back).  Each class runs the base-2 test
-//            in batches of 32 that are uniform in kind and nearly so in exponent length, the
+//            device work queue, trial-divide them, and file the survivors in three size
+//            classes (below 2^62, [2^62, 2^63), above; mp_mont64.cuh runs a different product
+//            form for each).  Each class runs the base-2 test in batches of 32 that are uniform
+//            in kind and nearly so in exponent length, the
 //            passers are compacted with warp ballots, the Lucas test runs on them, and the
 //            warp writes the chunk's verdict words.  Warps never wait for one another.  The
 //            warps per CTA and candidates per chunk are picked by the autotuner.
@@ -80,36 +80,53 @@ __global__ void __launch_bounds__(BPSW_WARPS * 32) bpsw_batched_kernel(const u64
         const u64 c0 = (u64)c * BPSW_WCHUNK;
         const u32 len = (u32)(total - c0 < BPSW_WCHUNK ? total - c0 : BPSW_WCHUNK);
         const u64 *nc = n + c0;
-        // 1. trial division: verdict words of the decided candidates; survivors filed by class
-        u32 ns = 0, nl = 0;
+        // 1. trial division: verdict words of the decided candidates; survivors filed by size
+        //    class: below 2^62 at the front of idx, [2^62, 2^63) at its back, 2^63 and above at
+        //    the front of pas (free until the base-2 passers are collected)
+        u32 ns = 0, nm = 0, nw = 0;
         for (u32 base = 0; base < len; base += 32) {
             const u32 i = base + lane;
             const u64 x = i < len ? __ldg(nc + i) : 0;
             const int v = i < len ? td_verdict(x) : 0;
             const u32 pm = __ballot_sync(0xffffffffu, v == 1);
-            const bool sm = v < 0 && x < BPSW_LAZY_MAX, lg = v < 0 && x >= BPSW_LAZY_MAX;
-            const u32 ms = __ballot_sync(0xffffffffu, sm), ml = __ballot_sync(0xffffffffu, lg);
+            const int c = spsp2_class(x);
+            const bool cs = v < 0 && c == SP_LAZY, cm = v < 0 && c == SP_FOLD, cw = v < 0 && c == SP_WIDE;
+            const u32 ms = __ballot_sync(0xffffffffu, cs), mm = __ballot_sync(0xffffffffu, cm);
+            const u32 mw = __ballot_sync(0xffffffffu, cw);
             if (lane == 0) wb[base >> 5] = pm;
-            if (sm) idx[ns + __popc(ms & lt)] = (u16)i;
-            if (lg) idx[BPSW_WCHUNK - 1 - (nl + __popc(ml & lt))] = (u16)i;
+            if (cs) idx[ns + __popc(ms & lt)] = (u16)i;
+            if (cm) idx[BPSW_WCHUNK - 1 - (nm + __popc(mm & lt))] = (u16)i;
+            if (cw) pas[nw + __popc(mw & lt)] = (u16)i;
             ns += __popc(ms);
-            nl += __popc(ml);
+            nm += __popc(mm);
+            nw += __popc(mw);
         }
         __syncwarp();
-        // 2. base-2 strong test, one class after the other; passers compacted into pas
+        // 2. base-2 strong test, one class after the other; the passers are compacted to the
+        //    front of pas.  The widest class goes first: it is read from pas, and a batch's
+        //    passers are written only after every lane has read its entry (np <= base)
         u32 np = 0;
-        for (u32 base = 0; base < ns; base += 32) {
+        for (u32 base = 0; base < nw; base += 32) {
             const u32 k = base + lane;
-            const u32 i = k < ns ? idx[k] : 0;
-            const bool pass = k < ns && spsp2<true>(mm_setup(__ldg(nc + i)));
+            const u32 i = k < nw ? pas[k] : 0;
+            const bool pass = k < nw && spsp2<SP_WIDE>(mm_setup(__ldg(nc + i)));
+            const u32 m = __ballot_sync(0xffffffffu, pass);
+            if (pass) pas[np + __popc(m & lt)] = (u16)i;
+            np += __popc(m);
+            __syncwarp();
+        }
+        for (u32 base = 0; base < nm; base += 32) {
+            const u32 k = base + lane;
+            const u32 i = k < nm ? idx[BPSW_WCHUNK - 1 - k] : 0;
+            const bool pass = k < nm && spsp2<SP_FOLD>(mm_setup(__ldg(nc + i)));
             const u32 m = __ballot_sync(0xffffffffu, pass);
             if (pass) pas[np + __popc(m & lt)] = (u16)i;
             np += __popc(m);
         }
-        for (u32 base = 0; base < nl; base += 32) {
+        for (u32 base = 0; base < ns; base += 32) {
             const u32 k = base + lane;
-            const u32 i = k < nl ? idx[BPSW_WCHUNK - 1 - k] : 0;
-            const bool pass = k < nl && spsp2<false>(mm_setup(__ldg(nc + i)));
+            const u32 i = k < ns ? idx[k] : 0;
+            const bool pass = k < ns && spsp2<SP_LAZY>(mm_setup(__ldg(nc + i)));
             const u32 m = __ballot_sync(0xffffffffu, pass);
             if (pass) pas[np + __popc(m & lt)] = (u16)i;
             np += __popc(m);
@@ -124,8 +141,8 @@ __global__ void __launch_bounds__(BPSW_WARPS * 32) bpsw_batched_kernel(const u64
             }
         }
         __syncwarp();
-        const u32 nw = (len + 31) / 32;
-        for (u32 w = lane; w < nw; w += 32) bits[(c0 >> 5) + w] = wb[w];
+        const u32 nwords = (len + 31) / 32;
+        for (u32 w = lane; w < nwords; w += 32) bits[(c0 >> 5) + w] = wb[w];
         __syncwarp();
     }
 }

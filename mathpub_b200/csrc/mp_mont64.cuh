@@ -8,15 +8,19 @@
 // give exact primality below 2^64, so the verdicts are the reference's.  How it is computed is
 // this file's own design, from the published mathematics:
 //
-//  * A residue is two 32-bit limbs.  A product is the full 128-bit product followed by a
-//    word-by-word Montgomery reduction (R = 2^64; per word m = t_i (-n^-1) mod 2^32, t += m n
-//    2^(32 i)), each one PTX block of 32-bit multiply-add carry chains.
-//  * For n < 2^62 (so 4n <= R) residues stay in [0, 2n) and no product is followed by a
-//    subtraction (lazy reduction).  Above, every product ends with one conditional subtraction
-//    (the 129-bit sum keeps its carry word, so every odd n < 2^64 is handled).
-//  * Base-2 exponentiation, left to right: square, then multiply by 2^b for the exponent bit b
-//    as a funnel shift of the residue by b (0 or 1) and one conditional subtraction; no select
-//    between two candidate residues.
+//  * A residue is two 32-bit limbs; each product is one PTX block of 32-bit multiply-add carry
+//    chains.  Two reductions of the 128-bit product t (R = 2^64):
+//      - adding: word by word, m = t_i (-n^-1) mod 2^32, t += m n 2^(32 i).  For n < 2^62 (so
+//        4n <= R) residues stay in [0, 2n) with no subtraction after a product (lazy);
+//      - subtracting: m = t n^-1 mod 2^64, then (t - m n) / R = t_hi - hi(m n), exact since the
+//        low halves agree, plus n when it borrows.  In and out in [0, n), for any odd n; fewer
+//        carry adds than the adding form, and its input may be up to n R, which lets the
+//        doubling below fold into the product for n < 2^63.
+//  * Base-2 exponentiation, left to right, in three size classes (warps run one class at a
+//    time): n < 2^62, lazy adding products, then a doubling by a funnel shift of the residue by
+//    the exponent bit b and one conditional subtraction (no select between two residues);
+//    2^62 <= n < 2^63, one subtracting product x (x 2^b) per bit (below 2 n^2 < n R);
+//    n >= 2^63, a subtracting square, then the doubling.
 //  * Lucas sequences (P = 1, Q = (1 - D)/4) run as the ladder (V_k, V_k+1, Q^k) with
 //        V_2k = V_k^2 - 2 Q^k,   V_2k+1 = V_k V_k+1 - P Q^k,
 //    the same four products for either exponent bit (the bit only selects operands), so the
@@ -41,43 +45,15 @@ __host__ __device__ __forceinline__ u64 inv64(u64 n)
     return x;
 }
 
-// the modulus with what the products need: its limbs, -n^-1 mod 2^32, 2n, and R mod n
+// the modulus with what the products need: 2n, n^-1 mod 2^64, -n^-1 mod 2^32, and R mod n
 struct Mod64 {
     u64 n, n2;     // n and 2n (2n is used below 2^62 only)
+    u64 ni;        // n^-1 mod 2^64 (the subtracting reduction)
     u64 one;       // R mod n, the residue of 1
-    u32 np;        // -n^-1 mod 2^32
+    u32 np;        // -n^-1 mod 2^32 (the adding reduction)
 };
 
-// ---- products: t = a b (128 bits), then t += m0 n + m1 n 2^32, result t / 2^64 ----
-
-// the reduction tail shared by the products: t0..t3 hold a b; leaves the result in t2, t3 and
-// its carry word in t4 (0 or 1)
-#define MM_REDUCE_FULL                                   \
-    "mul.lo.u32     m, t0, %3;\n\t"                      \
-    "mad.lo.cc.u32  t0, m, n0, t0;\n\t"                  \
-    "madc.lo.cc.u32 t1, m, n1, t1;\n\t"                  \
-    "addc.cc.u32    t2, t2, 0;\n\t"                      \
-    "addc.cc.u32    t3, t3, 0;\n\t"                      \
-    "addc.u32       t4, 0, 0;\n\t"                       \
-    "mad.hi.cc.u32  t1, m, n0, t1;\n\t"                  \
-    "madc.hi.cc.u32 t2, m, n1, t2;\n\t"                  \
-    "addc.cc.u32    t3, t3, 0;\n\t"                      \
-    "addc.u32       t4, t4, 0;\n\t"                      \
-    "mul.lo.u32     m, t1, %3;\n\t"                      \
-    "mad.lo.cc.u32  t1, m, n0, t1;\n\t"                  \
-    "madc.lo.cc.u32 t2, m, n1, t2;\n\t"                  \
-    "addc.cc.u32    t3, t3, 0;\n\t"                      \
-    "addc.u32       t4, t4, 0;\n\t"                      \
-    "mad.hi.cc.u32  t2, m, n0, t2;\n\t"                  \
-    "madc.hi.cc.u32 t3, m, n1, t3;\n\t"                  \
-    "addc.u32       t4, t4, 0;\n\t"                      \
-    /* the result is below 2n: subtract n once when it is >= n (bw = 0) */ \
-    "sub.cc.u32     d0, t2, n0;\n\t"                     \
-    "subc.cc.u32    d1, t3, n1;\n\t"                     \
-    "subc.u32       bw, t4, 0;\n\t"                      \
-    "setp.ne.u32    p, bw, 0;\n\t"                       \
-    "selp.u32       t2, t2, d0, p;\n\t"                  \
-    "selp.u32       t3, t3, d1, p;\n\t"
+// ---- products: t = a b (128 bits), then one of the two reductions, result t / 2^64 ----
 
 // n < 2^62: every partial sum stays below 2^128 (a b < 4n^2 <= 2^126), so no carry word, and
 // the result (below 2n) is not reduced
@@ -97,59 +73,66 @@ struct Mod64 {
     "mad.hi.cc.u32  t2, m, n0, t2;\n\t"                  \
     "madc.hi.u32    t3, m, n1, t3;\n\t"
 
-#define MM_REGS ".reg .u32 a0, a1, b0, b1, n0, n1, t0, t1, t2, t3, t4, m, d0, d1, bw;\n\t.reg .pred p;\n\t"
+#define MM_REGS ".reg .u32 a0, a1, n0, n1, t0, t1, t2, t3, m;\n\t"
 
-// a^2 / R mod n.  LAZY (n < 2^62): a in [0, 2n), result in [0, 2n).  Otherwise a in [0, n),
-// result in [0, n).
-template <bool LAZY>
-__device__ __forceinline__ u64 mm_sqr(u64 a, const Mod64 &M)
-{
-    u64 r;
-    if (LAZY)
-        asm("{\n\t" MM_REGS
-            "mov.b64 {a0, a1}, %1;\n\t"
-            "mov.b64 {n0, n1}, %2;\n\t"
-            "mul.lo.u32     t0, a0, a0;\n\t"
-            "mul.hi.u32     t1, a0, a0;\n\t"
-            "mul.lo.u32     t2, a1, a1;\n\t"
-            "mul.hi.u32     t3, a1, a1;\n\t"
-            "mad.lo.cc.u32  t1, a0, a1, t1;\n\t"
-            "madc.hi.cc.u32 t2, a0, a1, t2;\n\t"
-            "addc.u32       t3, t3, 0;\n\t"
-            "mad.lo.cc.u32  t1, a0, a1, t1;\n\t"
-            "madc.hi.cc.u32 t2, a0, a1, t2;\n\t"
-            "addc.u32       t3, t3, 0;\n\t"
-            MM_REDUCE_LAZY
-            "mov.b64 %0, {t2, t3};\n\t}"
-            : "=l"(r) : "l"(a), "l"(M.n), "r"(M.np));
-    else
-        asm("{\n\t" MM_REGS
-            "mov.b64 {a0, a1}, %1;\n\t"
-            "mov.b64 {n0, n1}, %2;\n\t"
-            "mul.lo.u32     t0, a0, a0;\n\t"
-            "mul.hi.u32     t1, a0, a0;\n\t"
-            "mul.lo.u32     t2, a1, a1;\n\t"
-            "mul.hi.u32     t3, a1, a1;\n\t"
-            "mad.lo.cc.u32  t1, a0, a1, t1;\n\t"
-            "madc.hi.cc.u32 t2, a0, a1, t2;\n\t"
-            "addc.u32       t3, t3, 0;\n\t"
-            "mad.lo.cc.u32  t1, a0, a1, t1;\n\t"
-            "madc.hi.cc.u32 t2, a0, a1, t2;\n\t"
-            "addc.u32       t3, t3, 0;\n\t"
-            MM_REDUCE_FULL
-            "mov.b64 %0, {t2, t3};\n\t}"
-            : "=l"(r) : "l"(a), "l"(M.n), "r"(M.np));
-    return r;
-}
-
-// a b / R mod n for a, b in [0, n), result in [0, n)
-__device__ __forceinline__ u64 mm_mul(u64 a, u64 b, const Mod64 &M)
+// a^2 / R mod n by the lazy adding reduction, for n < 2^62: a in [0, 2n), result in [0, 2n)
+__device__ __forceinline__ u64 ml_sqr(u64 a, const Mod64 &M)
 {
     u64 r;
     asm("{\n\t" MM_REGS
         "mov.b64 {a0, a1}, %1;\n\t"
         "mov.b64 {n0, n1}, %2;\n\t"
-        "mov.b64 {b0, b1}, %4;\n\t"
+        "mul.lo.u32     t0, a0, a0;\n\t"
+        "mul.hi.u32     t1, a0, a0;\n\t"
+        "mul.lo.u32     t2, a1, a1;\n\t"
+        "mul.hi.u32     t3, a1, a1;\n\t"
+        "mad.lo.cc.u32  t1, a0, a1, t1;\n\t"
+        "madc.hi.cc.u32 t2, a0, a1, t2;\n\t"
+        "addc.u32       t3, t3, 0;\n\t"
+        "mad.lo.cc.u32  t1, a0, a1, t1;\n\t"
+        "madc.hi.cc.u32 t2, a0, a1, t2;\n\t"
+        "addc.u32       t3, t3, 0;\n\t"
+        MM_REDUCE_LAZY
+        "mov.b64 %0, {t2, t3};\n\t}"
+        : "=l"(r) : "l"(a), "l"(M.n), "r"(M.np));
+    return r;
+}
+
+// the subtracting reduction of t3:t2:t1:t0 (< n R): m = (t1:t0) n^-1 mod 2^64 (i1:i0), then
+// (t3:t2) - hi64(m n) + (n if it borrows).  The words of m n below 2^64 equal t1:t0, so only
+// their carries into word 2 are formed.
+#define MM_REDUCE_SUB                                    \
+    "mul.lo.u32     m0, t0, i0;\n\t"                     \
+    "mul.hi.u32     m1, t0, i0;\n\t"                     \
+    "mad.lo.u32     m1, t0, i1, m1;\n\t"                 \
+    "mad.lo.u32     m1, t1, i0, m1;\n\t"                 \
+    "mul.hi.u32     v1, m0, n0;\n\t"                     \
+    "mad.lo.cc.u32  v1, m0, n1, v1;\n\t"                 \
+    "madc.hi.u32    v2, m0, n1, 0;\n\t"                  \
+    "mad.lo.cc.u32  v1, m1, n0, v1;\n\t"                 \
+    "madc.hi.cc.u32 v2, m1, n0, v2;\n\t"                 \
+    "addc.u32       v3, 0, 0;\n\t"                       \
+    "mad.lo.cc.u32  v2, m1, n1, v2;\n\t"                 \
+    "madc.hi.u32    v3, m1, n1, v3;\n\t"                 \
+    "sub.cc.u32     t2, t2, v2;\n\t"                     \
+    "subc.cc.u32    t3, t3, v3;\n\t"                     \
+    "subc.u32       bw, 0, 0;\n\t"                       \
+    "and.b32        k0, n0, bw;\n\t"                     \
+    "and.b32        k1, n1, bw;\n\t"                     \
+    "add.cc.u32     t2, t2, k0;\n\t"                     \
+    "addc.u32       t3, t3, k1;\n\t"
+
+#define MS_REGS ".reg .u32 a0, a1, b0, b1, n0, n1, i0, i1, t0, t1, t2, t3, m0, m1, v1, v2, v3, bw, k0, k1;\n\t"
+
+// a b / R mod n by the subtracting reduction: a, b < n (or a b < n R), result in [0, n)
+__device__ __forceinline__ u64 ms_mul(u64 a, u64 b, const Mod64 &M)
+{
+    u64 r;
+    asm("{\n\t" MS_REGS
+        "mov.b64 {a0, a1}, %1;\n\t"
+        "mov.b64 {b0, b1}, %2;\n\t"
+        "mov.b64 {n0, n1}, %3;\n\t"
+        "mov.b64 {i0, i1}, %4;\n\t"
         "mul.lo.u32     t0, a0, b0;\n\t"
         "mul.hi.u32     t1, a0, b0;\n\t"
         "mul.lo.u32     t2, a1, b1;\n\t"
@@ -160,9 +143,33 @@ __device__ __forceinline__ u64 mm_mul(u64 a, u64 b, const Mod64 &M)
         "mad.lo.cc.u32  t1, a1, b0, t1;\n\t"
         "madc.hi.cc.u32 t2, a1, b0, t2;\n\t"
         "addc.u32       t3, t3, 0;\n\t"
-        MM_REDUCE_FULL
+        MM_REDUCE_SUB
         "mov.b64 %0, {t2, t3};\n\t}"
-        : "=l"(r) : "l"(a), "l"(M.n), "r"(M.np), "l"(b));
+        : "=l"(r) : "l"(a), "l"(b), "l"(M.n), "l"(M.ni));
+    return r;
+}
+
+// a^2 / R mod n by the subtracting reduction, a in [0, n)
+__device__ __forceinline__ u64 ms_sqr(u64 a, const Mod64 &M)
+{
+    u64 r;
+    asm("{\n\t" MS_REGS
+        "mov.b64 {a0, a1}, %1;\n\t"
+        "mov.b64 {n0, n1}, %2;\n\t"
+        "mov.b64 {i0, i1}, %3;\n\t"
+        "mul.lo.u32     t0, a0, a0;\n\t"
+        "mul.hi.u32     t1, a0, a0;\n\t"
+        "mul.lo.u32     t2, a1, a1;\n\t"
+        "mul.hi.u32     t3, a1, a1;\n\t"
+        "mad.lo.cc.u32  t1, a0, a1, t1;\n\t"
+        "madc.hi.cc.u32 t2, a0, a1, t2;\n\t"
+        "addc.u32       t3, t3, 0;\n\t"
+        "mad.lo.cc.u32  t1, a0, a1, t1;\n\t"
+        "madc.hi.cc.u32 t2, a0, a1, t2;\n\t"
+        "addc.u32       t3, t3, 0;\n\t"
+        MM_REDUCE_SUB
+        "mov.b64 %0, {t2, t3};\n\t}"
+        : "=l"(r) : "l"(a), "l"(M.n), "l"(M.ni));
     return r;
 }
 
@@ -230,7 +237,8 @@ __device__ __forceinline__ Mod64 mm_setup(u64 n)
     Mod64 M;
     M.n = n;
     M.n2 = n << 1;
-    M.np = 0u - (u32)inv64(n);
+    M.ni = inv64(n);
+    M.np = 0u - (u32)M.ni;
     const int top = 63 - __clzll((long long)n);
     u64 x = 1ull << top;
     for (int i = top; i < 64; i++) x = mm_dbl<false>(x, 1u, M);
@@ -253,9 +261,17 @@ __device__ __forceinline__ u64 mm_from_small(i32 v, const Mod64 &M)
 
 // ---- base-2 strong probable-prime test ----
 
+// size classes of the base-2 ladder: below 2^62 (lazy adding products), [2^62, 2^63) (the
+// doubling folded into a subtracting product), 2^63 and above (subtracting square, doubling)
+#define SP_LAZY 0
+#define SP_FOLD 1
+#define SP_WIDE 2
+
+__device__ __forceinline__ int spsp2_class(u64 n) { return n < (1ull << 62) ? SP_LAZY : n < (1ull << 63) ? SP_FOLD : SP_WIDE; }
+
 // n - 1 = d 2^s with d odd: 2^d (mod n) by the left-to-right ladder, then the strong
-// condition 2^d = 1, or 2^(d 2^r) = -1 for some 0 <= r < s.  Odd n > 2.
-template <bool LAZY>
+// condition 2^d = 1, or 2^(d 2^r) = -1 for some 0 <= r < s.  Odd n > 2 in size class CLS.
+template <int CLS>
 __device__ __forceinline__ bool spsp2(const Mod64 &M)
 {
     const u64 n = M.n;
@@ -264,26 +280,35 @@ __device__ __forceinline__ bool spsp2(const Mod64 &M)
     const int L = 63 - __clzll((long long)d);               // d's top bit: the ladder starts at 2
     u64 x = mm_dbl<false>(M.one, 1u, M);
     for (int i = L - 1; i >= 0; i--) {
-        x = mm_sqr<LAZY>(x, M);
-        x = mm_dbl<LAZY>(x, (u32)(d >> i) & 1u, M);
+        const u32 bit = (u32)(d >> i) & 1u;
+        if (CLS == SP_LAZY) {
+            x = ml_sqr(x, M);
+            x = mm_dbl<true>(x, bit, M);
+        } else if (CLS == SP_FOLD) {
+            x = ms_mul(x, x << bit, M);                     // x (x 2^bit) / R < 2 n^2 / R < n
+        } else {
+            x = ms_sqr(x, M);
+            x = mm_dbl<false>(x, bit, M);
+        }
     }
     const u64 mone = n - M.one;                             // the residue of -1
-    if (LAZY) x = mm_canon(x, n);
+    if (CLS == SP_LAZY) x = mm_canon(x, n);
     bool pass = x == M.one || x == mone;
     for (int r = 1; r < s && !pass; r++) {
         if (x == M.one) break;                              // 1 before -1: not a strong probable prime
-        x = mm_sqr<LAZY>(x, M);
-        if (LAZY) x = mm_canon(x, n);
+        if (CLS == SP_LAZY) x = mm_canon(ml_sqr(x, M), n);
+        else x = ms_sqr(x, M);
         pass = x == mone;
     }
     return pass;
 }
 
-// the test for any odd n > 2, with the lazy form chosen by size
+// the test for any odd n > 2, in its size class
 __device__ __forceinline__ bool spsp2_u64(u64 n)
 {
     const Mod64 M = mm_setup(n);
-    return n < (1ull << 62) ? spsp2<true>(M) : spsp2<false>(M);
+    const int c = spsp2_class(n);
+    return c == SP_LAZY ? spsp2<SP_LAZY>(M) : c == SP_FOLD ? spsp2<SP_FOLD>(M) : spsp2<SP_WIDE>(M);
 }
 
 // ---- strong Lucas test ----
@@ -363,19 +388,19 @@ __device__ __forceinline__ bool lucas_strong(const Mod64 &M, i32 D)
     u64 qk = q1;
     for (int i = 62 - __clzll((long long)d); i >= 0; i--) {
         const bool b = (d >> i) & 1;
-        const u64 w = mm_sub(mm_mul(vk, vk1, M), qk, n);               // V_2k+1
-        const u64 qb = mm_mul(qk, b ? q1 : M.one, M);                  // Q^(k+b)
-        const u64 sq = mm_sqr<false>(b ? vk1 : vk, M);
+        const u64 w = mm_sub(ms_mul(vk, vk1, M), qk, n);               // V_2k+1
+        const u64 qb = ms_mul(qk, b ? q1 : M.one, M);                  // Q^(k+b)
+        const u64 sq = ms_sqr(b ? vk1 : vk, M);
         const u64 v2 = mm_sub(sq, mm_add(qb, qb, n), n);               // V_2(k+b)
-        qk = mm_mul(qk, qb, M);                                        // Q^(2k+b)
+        qk = ms_mul(qk, qb, M);                                        // Q^(2k+b)
         vk = b ? w : v2;
         vk1 = b ? v2 : w;
     }
     if (vk == 0 || mm_add(vk1, vk1, n) == vk) return true;             // V_d = 0 or U_d = 0
     for (int r = 1; r < s; r++) {
-        vk = mm_sub(mm_sqr<false>(vk, M), mm_add(qk, qk, n), n);        // V_(d 2^r)
+        vk = mm_sub(ms_sqr(vk, M), mm_add(qk, qk, n), n);               // V_(d 2^r)
         if (vk == 0) return true;
-        qk = mm_sqr<false>(qk, M);
+        qk = ms_sqr(qk, M);
     }
     return false;
 }
@@ -395,7 +420,8 @@ __device__ __forceinline__ bool bpsw_odd(u64 n)
 {
     if (n == ~0ull) return false;
     const Mod64 M = mm_setup(n);
-    const bool p2 = n < (1ull << 62) ? spsp2<true>(M) : spsp2<false>(M);
+    const int c = spsp2_class(n);
+    const bool p2 = c == SP_LAZY ? spsp2<SP_LAZY>(M) : c == SP_FOLD ? spsp2<SP_FOLD>(M) : spsp2<SP_WIDE>(M);
     if (!p2) return false;
     const i32 D = selfridge_d(n);
     return D && lucas_strong(M, D);

@@ -1548,13 +1548,30 @@ static cudaError_t pipeline_ctas_per_sm(int nth, size_t smem, int *per_sm)
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, sieve_pipeline_kernel<TLOG>, nth, smem);
 }
 
+// the pipeline kernel's static shared memory (its tile scans and scatter counters)
+template <int TLOG>
+static cudaError_t pipeline_static_smem(size_t *bytes)
+{
+    cudaFuncAttributes fa;
+    const cudaError_t e = cudaFuncGetAttributes(&fa, sieve_pipeline_kernel<TLOG>);
+    if (e == cudaSuccess) *bytes = fa.sharedSizeBytes;
+    return e;
+}
+
 // the batched form in one persistent launch (sieve_pipeline_kernel): every wave's scatter and
 // tile items from one device queue, the records in a ring of two wave slots
-static int run_pipeline(mp_handle *h, const PrimeTable &tb, const SievePlan &P, TileArgs a, u32 binc, int smem_max,
+static int run_pipeline(mp_handle *h, const PrimeTable &tb, const SievePlan &P, TileArgs a, int smem_max,
                         int grid_pers, cudaStream_t st)
 {
     const int nth = P.nth;
     const u32 tlog = P.g.tlog, nw = P.nwaves;
+    // the dynamic shared memory left beside the kernel's static shared memory bounds the bins
+    size_t stat = 0;
+    MP_CUDA(h, tlog == 18 ? pipeline_static_smem<18>(&stat) : tlog == 19 ? pipeline_static_smem<19>(&stat)
+                                                                         : pipeline_static_smem<20>(&stat));
+    smem_max = smem_max + 1024 - (int)stat - 256;
+    const u32 binc = binned_capacity(P.wt, smem_max);
+    if (!binc) return mp_set_error(h, MP_EINVAL, "the pipeline's scatter bins do not fit in shared memory");
     const size_t tile_smem = ((1u << tlog) / 32 + HALO_WORDS) * 4;
     const size_t scat_smem = ((size_t)P.wt * binc + P.wt + SB_OVF) * 4;
     const size_t smem = std::max(tile_smem, scat_smem);
@@ -1626,7 +1643,7 @@ static int run_tiles(mp_handle *h, const PrimeTable &tb, const SievePlan &P, Til
     smem_max -= 1024;                                   // the kernel's static shared memory and slack
     const u32 binc = P.large && h->tune.scatter_staged == 0 ? binned_capacity(wmax, smem_max) : 0u;
     if (P.large) MP_TRY(scatter_bounds(h, tb, P.ti.it1, P.ti.iend, binc ? 1u : (u32)SC_CTAS_PER_SM, st));
-    if (mode == 0 && !emit && binc && !h->tune.no_pipeline) return run_pipeline(h, tb, P, a, binc, smem_max, grid_pers, st);
+    if (mode == 0 && !emit && binc && !h->tune.no_pipeline) return run_pipeline(h, tb, P, a, smem_max, grid_pers, st);
     for (u32 L = 0; L < nlaunch; L++) {
         const u32 t0 = L * wmax;
         const u32 nt = std::min(wmax, P.g.ntiles - t0);
