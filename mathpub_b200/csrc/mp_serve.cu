@@ -4,8 +4,9 @@
 // that uses the server's resident sieving-prime table and presieve patterns, built once at
 // open for every height the server accepts.  Requests wait in one FIFO.  A worker takes
 // the next request when an in-flight slot is free and the request's device-memory estimate
-// fits in what the budget has left (admission by free device memory), so requests that
-// arrive while others are on the GPU are admitted as soon as slots and memory free up.
+// fits in what is left of the device's free memory, read with cudaMemGetInfo at admission
+// time (and of the option's cap), so requests that arrive while others are on the GPU are
+// admitted as soon as slots and memory free up.
 //   range request      runs the batched sieve on the worker's stream, at most `chunk`
 //                      integers at a time: a longer range goes back to the end of the queue
 //                      after each chunk (processor sharing), so that the short requests
@@ -49,7 +50,10 @@ struct mp_server {
     std::unordered_map<u64, ServeReq *> reqs;
     u64 next_id = 1;
     bool closing = false;
-    u64 budget = 0, mem_used = 0;
+    u64 budget = 0, mem_used = 0;    // budget: the cap from the options (or half the free HBM at open)
+    u64 free_hbm = 0;                // device free memory, last read
+    double free_at = 0;              // when it was read (seconds)
+    u64 reserve = 256ull << 20;      // free HBM never handed out
     u32 max_inflight = 256, inflight = 0;
     u64 prime_limit = 0;
     u64 chunk = 1ull << 32;          // least integers of a range request per turn
@@ -105,8 +109,27 @@ static void run_bpsw(mp_handle *w, std::vector<ServeReq *> &batch)
     for (ServeReq *r : batch) r->res.status = rc;
 }
 
+// the bytes of in-flight requests the server may hold now: the option's cap, and no more than
+// the device's free memory (cudaMemGetInfo, read again when the last reading is over 5 ms old)
+// less a reserve.  The workers' scratch was allocated at open, so the reading also tracks what
+// other processes on the device take.  Called with s->mu held.
+static u64 admit_limit(mp_server *s)
+{
+    const double t = now_s();
+    if (t - s->free_at > 0.005) {
+        size_t fr = 0, tot = 0;
+        if (cudaMemGetInfo(&fr, &tot) == cudaSuccess) {
+            s->free_hbm = fr;
+            s->free_at = t;
+        }
+    }
+    const u64 by_free = s->free_hbm > s->reserve ? s->free_hbm - s->reserve : 0;
+    return std::min(s->budget, by_free);
+}
+
 static void worker_loop(mp_server *s, mp_handle *w)
 {
+    cudaSetDevice(w->device);
     for (;;) {
         std::vector<ServeReq *> take;
         {
@@ -115,8 +138,9 @@ static void worker_loop(mp_server *s, mp_handle *w)
                 if (s->closing && s->pending.empty()) return;
                 if (!s->pending.empty() && s->inflight < s->max_inflight) {
                     ServeReq *head = s->pending.front();
-                    // admission: the head always fits when nothing else holds memory
-                    if (s->mem_used + head->mem <= s->budget || s->mem_used == 0) break;
+                    // admission by free device memory; the head always fits when nothing else
+                    // holds memory (a single request larger than the limit still runs, alone)
+                    if (s->mem_used + head->mem <= admit_limit(s) || s->mem_used == 0) break;
                 }
                 s->cv_work.wait_for(lk, std::chrono::milliseconds(50));
             }
@@ -130,7 +154,7 @@ static void worker_loop(mp_server *s, mp_handle *w)
                 for (auto it = s->pending.begin(); it != s->pending.end();) {
                     ServeReq *r = *it;
                     if (r->kind == 2 && (take.empty() || (cand + r->cand.size() <= s->bpsw_cap &&
-                                                         s->mem_used + r->mem <= s->budget &&
+                                                         s->mem_used + r->mem <= admit_limit(s) &&
                                                          s->inflight + take.size() < s->max_inflight))) {
                         cand += r->cand.size();
                         take.push_back(r);
