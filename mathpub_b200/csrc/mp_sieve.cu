@@ -1526,25 +1526,28 @@ static int scatter_bounds(mp_handle *h, const PrimeTable &tb, u32 i0, u32 i1, u3
 }
 
 template <int TLOG>
-static cudaError_t launch_pipeline(const PipeArgs &p, int grid, int nth, size_t smem, int smem_max, cudaStream_t st)
+static cudaError_t launch_pipeline(const PipeArgs &p, int grid, int nth, size_t smem, cudaStream_t st)
 {
-    static bool attr_set[16] = {false};
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev < 0 || dev >= 16) return cudaErrorInvalidDevice;
-    if (!attr_set[dev]) {
-        cudaError_t e = cudaFuncSetAttribute(sieve_pipeline_kernel<TLOG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             smem_max);
-        if (e != cudaSuccess) return e;
-        attr_set[dev] = true;
-    }
     sieve_pipeline_kernel<TLOG><<<grid, nth, smem, st>>>(p);
     return cudaGetLastError();
 }
 
+// resident CTAs per SM at `smem` bytes of dynamic shared memory, after raising the kernel's
+// limit on dynamic shared memory to `smem_max` (the occupancy calculation honours that limit,
+// so it is set first)
 template <int TLOG>
-static cudaError_t pipeline_ctas_per_sm(int nth, size_t smem, int *per_sm)
+static cudaError_t pipeline_ctas_per_sm(int nth, size_t smem, int smem_max, int *per_sm)
 {
+    static int attr_set[16] = {0};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 16) return cudaErrorInvalidDevice;
+    if (attr_set[dev] != smem_max) {
+        e = cudaFuncSetAttribute(sieve_pipeline_kernel<TLOG>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+        if (e != cudaSuccess) return e;
+        attr_set[dev] = smem_max;
+    }
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, sieve_pipeline_kernel<TLOG>, nth, smem);
 }
 
@@ -1576,9 +1579,9 @@ static int run_pipeline(mp_handle *h, const PrimeTable &tb, const SievePlan &P, 
     const size_t scat_smem = ((size_t)P.wt * binc + P.wt + SB_OVF) * 4;
     const size_t smem = std::max(tile_smem, scat_smem);
     int per_sm = 0;
-    cudaError_t e = tlog == 18 ? pipeline_ctas_per_sm<18>(nth, smem, &per_sm)
-                  : tlog == 19 ? pipeline_ctas_per_sm<19>(nth, smem, &per_sm)
-                               : pipeline_ctas_per_sm<20>(nth, smem, &per_sm);
+    cudaError_t e = tlog == 18 ? pipeline_ctas_per_sm<18>(nth, smem, smem_max, &per_sm)
+                  : tlog == 19 ? pipeline_ctas_per_sm<19>(nth, smem, smem_max, &per_sm)
+                               : pipeline_ctas_per_sm<20>(nth, smem, smem_max, &per_sm);
     MP_CUDA(h, e);
     if (per_sm < 1) return mp_set_error(h, MP_EINVAL, "the pipeline kernel does not fit on an SM");
     const int grid = h->sm_count * per_sm;
@@ -1609,9 +1612,9 @@ static int run_pipeline(mp_handle *h, const PrimeTable &tb, const SievePlan &P, 
     p.ctl = cnt0 + 2 * P.wt;
     p.spin_limit = 1u << 23;
     ProfScope ps(h, PROF_PIPELINE, st);
-    e = tlog == 18 ? launch_pipeline<18>(p, grid, nth, smem, smem_max, st)
-      : tlog == 19 ? launch_pipeline<19>(p, grid, nth, smem, smem_max, st)
-                   : launch_pipeline<20>(p, grid, nth, smem, smem_max, st);
+    e = tlog == 18 ? launch_pipeline<18>(p, grid, nth, smem, st)
+      : tlog == 19 ? launch_pipeline<19>(p, grid, nth, smem, st)
+                   : launch_pipeline<20>(p, grid, nth, smem, st);
     MP_CUDA(h, e);
     return MP_OK;
 }
