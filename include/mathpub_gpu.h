@@ -292,6 +292,27 @@ int mp_wieferich_stats_noalloc(const uint64_t *d_p, const uint64_t *d_q, uint64_
  * given height.  *report receives a short text summary (nullable, cap bytes). */
 int mp_autotune(mp_handle *h, uint64_t lo, char *report, size_t cap);
 
+/* Sets one of the autotuner's choices on the handle, as mp_autotune would (so that callers
+ * and tests can pin each one):
+ *   MP_TUNE_TILE_LOG2      sieve tile bits (0 = default, 18, 19, 20)
+ *   MP_TUNE_THREADS        sieve threads per CTA (0 = default, 256, 512, 1024)
+ *   MP_TUNE_SCATTER_STAGED 1: the staged bucket scatter, 0: the binned one
+ *   MP_TUNE_BUCKET_DIV     primes above tile bits / value (1, 2 or 4) go to the buckets
+ *   MP_TUNE_NO_PIPELINE    1: batched sieve calls as a host loop of wave launches, 0: one
+ *                          persistent pipeline launch
+ *   MP_TUNE_BPSW_VARIANT   0..3: warps x candidates per chunk of the batched BPSW kernel
+ *   MP_TUNE_FERMAT_ILP2    1: two primes per thread in the Fermat kernel
+ * Returns MP_EINVAL for an unknown knob or a value out of range.  No reference counterpart
+ * (the reference picks its wheel and chunk by a cost model, A350826/a350826.c:1976-2015). */
+#define MP_TUNE_TILE_LOG2 1
+#define MP_TUNE_THREADS 2
+#define MP_TUNE_SCATTER_STAGED 3
+#define MP_TUNE_BUCKET_DIV 4
+#define MP_TUNE_NO_PIPELINE 5
+#define MP_TUNE_BPSW_VARIANT 6
+#define MP_TUNE_FERMAT_ILP2 7
+int mp_tune_set(mp_handle *h, int knob, int value);
+
 /* ---- measurement ----
  * mp_profile_enable(h, 1) brackets every launch of the timed kernels with CUDA events on the
  * stream it runs on (batched sieve calls then run directly instead of replaying a captured

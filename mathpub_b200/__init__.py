@@ -127,6 +127,7 @@ def lib():
             "mp_chain_sieve128": ([vp, vp, vp, u32, u32, vp, vp, C.c_size_t, C.POINTER(C.c_size_t)], C.c_int),
             "mp_chain_first128": ([vp, vp, vp, u32, u32, vp, vp, C.POINTER(u32)], C.c_int),
             "mp_autotune": ([vp, u64, C.c_char_p, C.c_size_t], C.c_int),
+            "mp_tune_set": ([vp, C.c_int, C.c_int], C.c_int),
             "mp_profile_enable": ([vp, C.c_int], C.c_int),
             "mp_profile_read": ([vp, vp, vp, C.c_int], C.c_int),
             "mp_probe_peaks": ([vp] + [C.POINTER(C.c_double)] * 4, C.c_int),
@@ -369,6 +370,14 @@ class Engine:
         self._check(lib().mp_probe_peaks(self._h, C.byref(a), C.byref(b), C.byref(c), C.byref(d)))
         return {"smem_atomic_conflict_free": a.value, "smem_atomic_random": b.value, "imad32": c.value,
                 "l2_atomic_random": d.value}
+
+    TUNE_KNOBS = {"tile_log2": 1, "threads": 2, "scatter_staged": 3, "bucket_div": 4, "no_pipeline": 5,
+                  "bpsw_variant": 6, "fermat_ilp2": 7}
+
+    def tune_set(self, **knobs):
+        """Pin autotuner choices on this engine, e.g. tune_set(bucket_div=2, no_pipeline=1)."""
+        for k, v in knobs.items():
+            self._check(lib().mp_tune_set(self._h, self.TUNE_KNOBS[k], int(v)))
 
     def autotune(self, lo=10**15):
         buf = C.create_string_buffer(4096)

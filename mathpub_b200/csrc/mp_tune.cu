@@ -153,3 +153,42 @@ extern "C" int mp_autotune(mp_handle *h, uint64_t lo, char *report, size_t cap)
     }
     return MP_OK;
 }
+
+extern "C" int mp_tune_set(mp_handle *h, int knob, int value)
+{
+    if (!h) return MP_EINVAL;
+    std::lock_guard<std::recursive_mutex> lk(h->mu);
+    switch (knob) {
+    case MP_TUNE_TILE_LOG2:
+        if (value != 0 && (value < 18 || value > 20)) return MP_EINVAL;
+        h->tune.sieve_tile_log2 = value;
+        break;
+    case MP_TUNE_THREADS:
+        if (value != 0 && value != 256 && value != 512 && value != 1024) return MP_EINVAL;
+        h->tune.sieve_threads = value;
+        break;
+    case MP_TUNE_SCATTER_STAGED:
+        if (value != 0 && value != 1) return MP_EINVAL;
+        h->tune.scatter_staged = value;
+        break;
+    case MP_TUNE_BUCKET_DIV:
+        if (value != 1 && value != 2 && value != 4) return MP_EINVAL;
+        h->tune.bucket_div = value;
+        break;
+    case MP_TUNE_NO_PIPELINE:
+        if (value != 0 && value != 1) return MP_EINVAL;
+        h->tune.no_pipeline = value;
+        break;
+    case MP_TUNE_BPSW_VARIANT:
+        if (value < 0 || value > 3) return MP_EINVAL;
+        h->tune.bpsw_variant = value;
+        break;
+    case MP_TUNE_FERMAT_ILP2:
+        if (value != 0 && value != 1) return MP_EINVAL;
+        h->tune.fermat_variant = value ? 2 : 0;
+        break;
+    default:
+        return MP_EINVAL;
+    }
+    return MP_OK;
+}
