@@ -428,7 +428,7 @@ def run_ours(args):
             "chains": chains,
             "tuples": tuples,
             "serving": serving,
-            "autotune": tune_report.strip().splitlines()[-3:] if tune_report != "off" else "off",
+            "autotune": [s for s in tune_report.strip().splitlines() if "choice" in s] if tune_report != "off" else "off",
             "probes": peaks,
             "results": res, "results_job": res_job if world > 1 else None,
             "results_match_fixture": (res == ref_fixture) if (ref_fixture and rank == 0 and lo == LO) else None,

@@ -21,6 +21,7 @@
 // request has its own outputs; only scheduling differs.
 #include "mp_common.cuh"
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <deque>
@@ -51,8 +52,9 @@ struct mp_server {
     u64 next_id = 1;
     bool closing = false;
     u64 budget = 0, mem_used = 0;    // budget: the cap from the options (or half the free HBM at open)
-    u64 free_hbm = 0;                // device free memory, last read
-    double free_at = 0;              // when it was read (seconds)
+    std::atomic<u64> free_hbm{0};    // device free memory, last read (outside the lock)
+    std::atomic<double> free_at{0};  // when it was read (seconds)
+    std::atomic<int> reading{0};     // a worker is reading it now
     u64 reserve = 256ull << 20;      // free HBM never handed out
     u32 max_inflight = 256, inflight = 0;
     u64 prime_limit = 0;
@@ -109,21 +111,28 @@ static void run_bpsw(mp_handle *w, std::vector<ServeReq *> &batch)
     for (ServeReq *r : batch) r->res.status = rc;
 }
 
-// the bytes of in-flight requests the server may hold now: the option's cap, and no more than
-// the device's free memory (cudaMemGetInfo, read again when the last reading is over 5 ms old)
-// less a reserve.  The workers' scratch was allocated at open, so the reading also tracks what
-// other processes on the device take.  Called with s->mu held.
-static u64 admit_limit(mp_server *s)
+// the device's free memory, read again with cudaMemGetInfo when the last reading is over
+// 20 ms old, by one worker at a time and never under the server's lock: the driver call can
+// wait behind other threads' copies, and under the lock that wait would hold up every worker
+// and every submission
+static void refresh_free(mp_server *s)
 {
-    const double t = now_s();
-    if (t - s->free_at > 0.005) {
-        size_t fr = 0, tot = 0;
-        if (cudaMemGetInfo(&fr, &tot) == cudaSuccess) {
-            s->free_hbm = fr;
-            s->free_at = t;
-        }
-    }
-    const u64 by_free = s->free_hbm > s->reserve ? s->free_hbm - s->reserve : 0;
+    if (now_s() - s->free_at.load(std::memory_order_relaxed) < 0.020) return;
+    int idle = 0;
+    if (!s->reading.compare_exchange_strong(idle, 1)) return;
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) == cudaSuccess) s->free_hbm.store(fr, std::memory_order_relaxed);
+    s->free_at.store(now_s(), std::memory_order_relaxed);
+    s->reading.store(0);
+}
+
+// the bytes of in-flight requests the server may hold now: the option's cap, and no more than
+// the device's free memory at the last reading less a reserve.  The workers' scratch was
+// allocated at open, so the reading also tracks what other processes on the device take.
+static u64 admit_limit(const mp_server *s)
+{
+    const u64 fr = s->free_hbm.load(std::memory_order_relaxed);
+    const u64 by_free = fr > s->reserve ? fr - s->reserve : 0;
     return std::min(s->budget, by_free);
 }
 
@@ -132,17 +141,28 @@ static void worker_loop(mp_server *s, mp_handle *w)
     cudaSetDevice(w->device);
     for (;;) {
         std::vector<ServeReq *> take;
+        refresh_free(s);
         {
             std::unique_lock<std::mutex> lk(s->mu);
             for (;;) {
                 if (s->closing && s->pending.empty()) return;
+                bool by_mem = false;
                 if (!s->pending.empty() && s->inflight < s->max_inflight) {
                     ServeReq *head = s->pending.front();
                     // admission by free device memory; the head always fits when nothing else
                     // holds memory (a single request larger than the limit still runs, alone)
                     if (s->mem_used + head->mem <= admit_limit(s) || s->mem_used == 0) break;
+                    by_mem = true;
                 }
-                s->cv_work.wait_for(lk, std::chrono::milliseconds(50));
+                if (by_mem) {
+                    // held back by memory: read it again (outside the lock) and look again soon
+                    lk.unlock();
+                    refresh_free(s);
+                    lk.lock();
+                    s->cv_work.wait_for(lk, std::chrono::milliseconds(2));
+                } else {
+                    s->cv_work.wait_for(lk, std::chrono::milliseconds(50));
+                }
             }
             ServeReq *head = s->pending.front();
             if (head->kind == 1) {
@@ -250,6 +270,9 @@ int mp_serve_open(mp_handle *h, const mp_serve_opts *opts, mp_server **out)
             }
         }
     }
+    // the first reading of free memory, with every worker's scratch in place
+    if (cudaMemGetInfo(&fr, &tot) == cudaSuccess) s->free_hbm.store(fr);
+    s->free_at.store(now_s());
     for (mp_handle *w : s->workers) s->threads.emplace_back(worker_loop, s, w);
     h->servers_open++;
     *out = s;

@@ -884,7 +884,10 @@ __device__ __forceinline__ void scatter_binned_run(const ScatterArgs &a, const W
             }
             have = jj[0] < span;
         }
-        const int more = __syncthreads_or(have);            // every append of the round is done
+        // every append of the round is done; the loop goes on while any thread holds a prime
+        // or still has primes to set up (a large prime often ends within one turn, so `have`
+        // alone would end the loop with primes left)
+        const int more = __syncthreads_or(have || k < k_end);
         if (!more) break;
         if (round % SB_FLUSH_ROUNDS == 0) sb_flush(a, W, bin, cnt, ovf, &s_novf, binc);
     }

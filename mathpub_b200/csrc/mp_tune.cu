@@ -109,6 +109,8 @@ extern "C" int mp_autotune(mp_handle *h, uint64_t lo, char *report, size_t cap)
         if (ms < fb) { fb = ms; fv = v; }
     }
     h->tune.fermat_variant = fv & 2;
+    snprintf(line, sizeof line, "fermat choice: %d prime(s)/thread\n", (fv & 2) ? 2 : 1);
+    rep += line;
     // batched BPSW: 2^20 seeded odd candidates (three in four in [2^62, 2^64), the rest in
     // [2^40, 2^62)), one list, each warps x chunk pair the kernel is built for
     {
