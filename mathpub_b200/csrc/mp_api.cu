@@ -26,10 +26,11 @@ struct GraphKey {
     mp_sieve_opts o;
     void *out, *blocks, *hash, *bitmap;
     cudaStream_t st;
+    u64 tune_gen;                    // the tuned plan (tile, threads, scatter form, threshold) it ran with
     bool operator==(const GraphKey &k) const
     {
         return lo == k.lo && hi == k.hi && !memcmp(&o, &k.o, sizeof o) && out == k.out && blocks == k.blocks &&
-               hash == k.hash && bitmap == k.bitmap && st == k.st;
+               hash == k.hash && bitmap == k.bitmap && st == k.st && tune_gen == k.tune_gen;
     }
 };
 
@@ -84,8 +85,9 @@ int mp_init(int device, mp_handle **out)
     h->graphs = new GraphCache();
     DevBuf *bufs[] = {&h->tilesum, &h->blockacc, &h->rec, &h->reccnt, &h->queue, &h->errflag, &h->scratch_bitmap,
                       &h->bpsw_n, &h->bpsw_bits, &h->ferm_p, &h->ferm_q, &h->ferm_part, &h->stats_out, &h->small_out,
-                      &h->boot.q, &h->boot.magic, &h->table.q, &h->table.magic, &h->scat_bounds, &h->tstate, &h->gap_acc};
+                      &h->boot.q, &h->boot.magic, &h->table.q, &h->table.magic, &h->tstate, &h->gap_acc};
     for (DevBuf *b : bufs) b->gen = &h->buf_gen;
+    for (auto &e : h->scat) e.buf.gen = &h->buf_gen;
     *out = h;
     return MP_OK;
 }
@@ -99,8 +101,9 @@ int mp_free(mp_handle *h)
     mp_chain_free(h);
     DevBuf *bufs[] = {&h->tilesum, &h->blockacc, &h->rec, &h->reccnt, &h->queue, &h->errflag, &h->scratch_bitmap,
                       &h->bpsw_n, &h->bpsw_bits, &h->ferm_p, &h->ferm_q, &h->ferm_part, &h->stats_out, &h->small_out,
-                      &h->boot.q, &h->boot.magic, &h->table.q, &h->table.magic, &h->scat_bounds, &h->tstate, &h->gap_acc};
+                      &h->boot.q, &h->boot.magic, &h->table.q, &h->table.magic, &h->tstate, &h->gap_acc};
     for (DevBuf *b : bufs) b->release();
+    for (auto &e : h->scat) e.buf.release();
     for (int p = 0; p < MP_NPAT; p++)
         if (!h->shared_tables && h->pat_ready && h->pat.d_words[p]) cudaFree(h->pat.d_words[p]);
     if (h->h_err) cudaFreeHost(h->h_err);
@@ -155,7 +158,7 @@ int mp_sieve_range_dev(mp_handle *h, uint64_t lo, uint64_t hi, const mp_sieve_op
     GraphKey key;
     memset(&key, 0, sizeof key);
     key.lo = lo; key.hi = hi; key.o = o; key.out = d_out; key.blocks = d_blocks; key.hash = d_hash;
-    key.bitmap = d_bitmap; key.st = st;
+    key.bitmap = d_bitmap; key.st = st; key.tune_gen = h->tune_gen;
     GraphCache *gc = h->graphs;
     for (auto &g : gc->e)
         if (g.exec && g.key == key && g.gen == h->buf_gen) {

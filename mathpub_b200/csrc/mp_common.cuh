@@ -169,7 +169,7 @@ struct Autotune {
     int sieve_threads = 0;
     int fermat_variant = 0;
     int bpsw_variant = 0;            // warps per CTA x candidates per chunk of the batched BPSW kernel
-    int scatter_staged = 0;          // 1: the staged (sorted) bucket scatter instead of the binned one
+    int scatter_staged = 1;          // 1: the staged (sorted) bucket scatter, 0: the binned one
     int bucket_div = 1;              // primes above tile bits / bucket_div (1, 2 or 4) go to the bucket scatter
     int no_pipeline = 0;             // 1: batched sieve calls as a host loop of wave launches
     u64 tuned_at = 0;
@@ -207,10 +207,22 @@ struct mp_handle {
 
     // scratch
     DevBuf tilesum, blockacc, rec, reccnt, queue, errflag, scratch_bitmap, bpsw_n, bpsw_bits,
-        ferm_p, ferm_q, ferm_part, stats_out, small_out, scat_bounds, tstate, gap_acc;
-    u64 scat_key[3] = {~0ull, ~0ull, ~0ull};   // (first, end, blocks) the bounds were built for
+        ferm_p, ferm_q, ferm_part, stats_out, small_out, tstate, gap_acc;
+    // CTA bounds of the bucket scatter, one buffer per (first prime, end prime, CTAs): a
+    // captured graph reads the buffer it was captured with, so a buffer's contents are never
+    // rewritten; the least recently used one is freed (which invalidates the graphs) when a
+    // new key needs room
+    struct ScatBounds {
+        u64 key[3] = {~0ull, ~0ull, ~0ull};
+        u32 nblk = 0;
+        u64 stamp = 0;
+        DevBuf buf;
+    };
+    static const int NSCAT = 8;
+    ScatBounds scat[NSCAT];
+    const ScatBounds *scat_cur = nullptr;   // the bounds of the sieve call in progress
+    u64 scat_clock = 0;
     std::vector<u32> scat_host;
-    u32 scat_nblk = 0;
     u32 *h_err = nullptr;            // pinned mirror of errflag
 
     Autotune tune;
@@ -218,6 +230,7 @@ struct mp_handle {
     ChainDev *chain = nullptr;
 
     u64 buf_gen = 0;                 // bumped by every scratch reallocation
+    u64 tune_gen = 0;                // bumped by every change of the tuned sieve plan
     bool prof_on = false;
     std::vector<ProfEv> prof;
     std::vector<cudaEvent_t> prof_pool;

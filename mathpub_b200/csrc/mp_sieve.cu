@@ -781,14 +781,17 @@ __global__ void __launch_bounds__(SC_THREADS, SC_CTAS_PER_SM) scatter_kernel(Sca
     scatter_flush(a, stage, sorted, hist, gb, &s_fill, s_wsum);
 }
 
-// The binned form of the same scatter (the default): one CTA of SB_THREADS threads per SM,
-// whose shared memory holds a bin of `binc` records per tile of the wave.  A record goes
-// straight into its tile's bin (one shared atomic for the slot), so no sort is needed: every
-// SB_FLUSH_ROUNDS rounds (the same round in every thread, so the decision is uniform) each
-// warp writes whole bins of its tiles as coalesced runs, with one global atomic per tile to
-// reserve the run in the bucket.  A record that finds its bin full goes to an overflow list,
-// and past that straight to its bucket with a global atomic of its own; results are exact
-// either way.
+// The binned form of the same scatter: one CTA of SB_THREADS threads per SM, whose shared
+// memory holds a bin of `binc` records per tile of the wave.  A record goes straight into its
+// tile's bin (one shared atomic for the slot), so no sort is needed: every SB_FLUSH_ROUNDS
+// rounds (the same round in every thread, so the decision is uniform) each warp writes whole
+// bins of its tiles as coalesced runs, with one global atomic per tile to reserve the run in
+// the bucket.  A record that finds its bin full goes to an overflow list, and past that
+// straight to its bucket with a global atomic of its own; results are exact either way.
+// Measured on B200 at 1e15 (2^34 integers) it is about 6x slower than the staged form: in a
+// round the CTA's threads walk primes of about the same size from the start of the wave, so
+// their hits crowd into the same few dozen tiles, whose bins overflow at once and send most
+// records down the overflow path.  The staged form sorts whatever arrives and is the default.
 #define SB_THREADS 1024
 #define SB_OVF 1024
 #define SB_FLUSH_ROUNDS 4
@@ -1495,13 +1498,22 @@ static cudaError_t launch_scatter_binned(const ScatterArgs &s, u32 nblk, u32 bin
 
 // CTA boundaries for the scatter kernel: contiguous runs of the large primes [i0, i1) of equal
 // work, where a prime's work is its expected hits in a wave (proportional to 1/q) plus its
-// set-up, worth about 8 hits in a wave of 2^30 bits.  SC_CTAS_PER_SM persistent CTAs per SM.  Built on
-// the host from the table's prefix sums of 1/q and uploaded once per prime range (never
-// inside a capture).
+// set-up, worth about 8 hits in a wave of 2^30 bits; per_sm persistent CTAs per SM.  Built on
+// the host from the table's prefix sums of 1/q and uploaded once per (i0, i1, CTAs) into a
+// buffer of its own (never inside a capture: a capture finds the bounds of its direct run).
+// Sets h->scat_cur.
 static int scatter_bounds(mp_handle *h, const PrimeTable &tb, u32 i0, u32 i1, u32 per_sm, cudaStream_t st)
 {
     const u32 want = (u32)std::max<u64>(1, std::min<u64>((u64)h->sm_count * per_sm, i1 - i0));
-    if (h->scat_key[0] == i0 && h->scat_key[1] == i1 && h->scat_key[2] == want && h->scat_nblk) return MP_OK;
+    mp_handle::ScatBounds *slot = &h->scat[0];
+    for (auto &e : h->scat) {
+        if (e.key[0] == i0 && e.key[1] == i1 && e.key[2] == want && e.nblk) {
+            e.stamp = ++h->scat_clock;
+            h->scat_cur = &e;
+            return MP_OK;
+        }
+        if (e.stamp < slot->stamp) slot = &e;
+    }
     if (tb.inv_prefix.size() < (size_t)i1 + 1) return mp_set_error(h, MP_EINVAL, "prime table has no prefix sums");
     const double c = 8.0 / ((double)(1u << 30) * 8.0 / 15.0);      // set-up, in units of 1/q
     auto W = [&](u32 i) { return tb.inv_prefix[i] + c * i; };
@@ -1520,11 +1532,18 @@ static int scatter_bounds(mp_handle *h, const PrimeTable &tb, u32 i0, u32 i1, u3
         b.push_back(lo);
     }
     b.push_back(i1);
-    MP_CUDA(h, h->scat_bounds.ensure(b.size() * 4));
-    MP_CUDA(h, cudaMemcpyAsync(h->scat_bounds.p, b.data(), b.size() * 4, cudaMemcpyHostToDevice, st));
+    // the evicted buffer may be in a cached graph: free it (that invalidates the graphs) and
+    // allocate the new one
+    slot->nblk = 0;
+    slot->key[0] = slot->key[1] = slot->key[2] = ~0ull;
+    slot->buf.release();
+    MP_CUDA(h, slot->buf.ensure(b.size() * 4));
+    MP_CUDA(h, cudaMemcpyAsync(slot->buf.p, b.data(), b.size() * 4, cudaMemcpyHostToDevice, st));
     MP_CUDA(h, cudaStreamSynchronize(st));
-    h->scat_key[0] = i0; h->scat_key[1] = i1; h->scat_key[2] = want;
-    h->scat_nblk = (u32)b.size() - 1;
+    slot->key[0] = i0; slot->key[1] = i1; slot->key[2] = want;
+    slot->nblk = (u32)b.size() - 1;
+    slot->stamp = ++h->scat_clock;
+    h->scat_cur = slot;
     return MP_OK;
 }
 
@@ -1602,10 +1621,10 @@ static int run_pipeline(mp_handle *h, const PrimeTable &tb, const SievePlan &P, 
     ScatterArgs &s = p.sa;
     s.base = P.g.base; s.tlog = tlog; s.nbx = P.g.nbx;
     s.q = tb.q.as<u32>(); s.magic = tb.magic.as<u64>();
-    s.bounds = h->scat_bounds.as<u32>();
+    s.bounds = h->scat_cur->buf.as<u32>();
     s.cap = P.cap; s.err = h->errflag.as<u32>();
     p.nwaves = nw; p.wt = P.wt; p.ntiles = P.g.ntiles;
-    p.nscat = h->scat_nblk;
+    p.nscat = h->scat_cur->nblk;
     p.run = std::max<u32>(1, P.wt / (u32)grid);
     p.binc = binc;
     p.rec[0] = h->rec.as<u32>();
@@ -1657,10 +1676,10 @@ static int run_tiles(mp_handle *h, const PrimeTable &tb, const SievePlan &P, Til
             ScatterArgs s;
             s.base = P.g.base; s.tlog = P.g.tlog; s.t0 = t0; s.wt = nt; s.nbx = P.g.nbx;
             s.q = tb.q.as<u32>(); s.magic = tb.magic.as<u64>();
-            s.bounds = h->scat_bounds.as<u32>();
+            s.bounds = h->scat_cur->buf.as<u32>();
             s.rec = h->rec.as<u32>(); s.cnt = h->reccnt.as<u32>(); s.cap = P.cap; s.err = errp;
             MP_CUDA(h, cudaMemsetAsync(s.cnt, 0, (size_t)nt * 4, st));
-            const u32 nblk = h->scat_nblk;
+            const u32 nblk = h->scat_cur->nblk;
             {
                 ProfScope ps(h, PROF_SCATTER, st);
                 if (binc) MP_CUDA(h, launch_scatter_binned(s, nblk, binc, smem_max, st));
@@ -1755,7 +1774,13 @@ int mp_tables_ensure(mp_handle *h, u64 limit)
     h->table.inv_prefix.resize(total + 1);
     h->table.inv_prefix[0] = 0.0;
     for (u64 i = 0; i < total; i++) h->table.inv_prefix[i + 1] = h->table.inv_prefix[i] + 1.0 / h->table.host[i];
-    h->scat_key[0] = ~0ull;
+    // the prime indices changed meaning: drop every scatter bound (and with them the graphs)
+    for (auto &e : h->scat) {
+        e.buf.release();
+        e.nblk = 0;
+        e.key[0] = e.key[1] = e.key[2] = ~0ull;
+    }
+    h->scat_cur = nullptr;
     MP_TRY(check_errflag(h, st));
     h->table.n = total;
     h->table.limit = L;

@@ -32,12 +32,15 @@ extern "C" int mp_autotune(mp_handle *h, uint64_t lo, char *report, size_t cap)
     MP_CUDA(h, cudaSetDevice(h->device));
     std::string rep;
     char line[160];
-    // sieve: a range of 2^32 integers at height lo
-    const u64 span = 1ull << 32;
+    // sieve: a range of 2^34 integers at height lo (several waves, as in long scans); a choice
+    // replaces the default only when it is more than 2% faster, so that timing noise between
+    // near-equal forms does not decide
+    const u64 span = 1ull << 34;
+    const float margin = 1.02f;
     if (lo > MP_HI_MAX - span) lo = MP_HI_MAX - span;
     MP_CUDA(h, h->small_out.ensure(4096));
     mp_range_stats *d_out = (mp_range_stats *)h->small_out.p;
-    float best = 1e30f;
+    float best = 1e30f, dflt = 1e30f;
     u32 bt = 20, bn = 1024;
     static const u32 tl[3] = {18, 19, 20}, th[3] = {256, 512, 1024};
     for (u32 a : tl)
@@ -45,39 +48,44 @@ extern "C" int mp_autotune(mp_handle *h, uint64_t lo, char *report, size_t cap)
             float ms = 0;
             const int r = time_sieve(h, lo, lo + span, a, b, d_out, &ms);
             if (r != MP_OK) return r;
-            snprintf(line, sizeof line, "sieve tile 2^%u x %u threads: %.3f ms / 2^32\n", a, b, ms / 3);
+            snprintf(line, sizeof line, "sieve tile 2^%u x %u threads: %.3f ms / 2^34\n", a, b, ms / 3);
             rep += line;
             if (ms < best) { best = ms; bt = a; bn = b; }
+            if (a == 20 && b == 1024) dflt = ms;
         }
+    if (dflt <= best * margin) { bt = 20; bn = 1024; }
     h->tune.sieve_tile_log2 = (int)bt;
     h->tune.sieve_threads = (int)bn;
     h->tune.tuned_at = lo;
-    // one knob at a time at that geometry, each against a 2^32-integer range:
-    //   the bucket scatter's form: binned (one CTA per SM, a bin per tile) or staged (three
-    //   CTAs per SM, a sorted stage);
+    h->tune_gen++;
+    // one knob at a time at that geometry, on the same range, the first value the default:
+    //   the bucket scatter's form: staged (three CTAs per SM, a sorted stage) or binned (one
+    //   CTA per SM, a bin per tile);
     //   the bucket threshold: primes above the tile size, half of it or a quarter of it go to
     //   the scatter (fewer visits of sparse primes per tile against more bucket records);
     //   the batched form as one persistent pipeline launch or as a host loop of wave launches
     struct Knob { const char *name; int *field; int vals[3]; int nv; const char *labels[3]; };
     Knob knobs[3] = {
-        {"scatter", &h->tune.scatter_staged, {0, 1, 0}, 2, {"binned", "staged", ""}},
+        {"scatter", &h->tune.scatter_staged, {1, 0, 0}, 2, {"staged", "binned", ""}},
         {"bucket threshold", &h->tune.bucket_div, {1, 2, 4}, 3, {"tile", "tile/2", "tile/4"}},
         {"batched form", &h->tune.no_pipeline, {0, 1, 0}, 2, {"pipeline", "wave loop", ""}},
     };
     for (Knob &k : knobs) {
-        float kb = 1e30f;
+        float kb = 1e30f, k0 = 1e30f;
         int kv = k.vals[0];
         for (int i = 0; i < k.nv; i++) {
             *k.field = k.vals[i];
             float ms = 0;
             const int r = time_sieve(h, lo, lo + span, bt, bn, d_out, &ms);
-            if (r != MP_OK) { *k.field = k.vals[0]; return r; }
-            snprintf(line, sizeof line, "%s %s: %.3f ms / 2^32\n", k.name, k.labels[i], ms / 3);
+            if (r != MP_OK) { *k.field = k.vals[0]; h->tune_gen++; return r; }
+            snprintf(line, sizeof line, "%s %s: %.3f ms / 2^34\n", k.name, k.labels[i], ms / 3);
             rep += line;
             if (ms < kb) { kb = ms; kv = k.vals[i]; }
+            if (i == 0) k0 = ms;
         }
-        *k.field = kv;
+        *k.field = k0 <= kb * margin ? k.vals[0] : kv;
     }
+    h->tune_gen++;
     snprintf(line, sizeof line, "sieve choice: tile 2^%u, %u threads, %s scatter, bucket threshold tile/%d, %s\n", bt,
              bn, h->tune.scatter_staged ? "staged" : "binned", h->tune.bucket_div,
              h->tune.no_pipeline ? "wave loop" : "pipeline");
@@ -192,5 +200,6 @@ extern "C" int mp_tune_set(mp_handle *h, int knob, int value)
     default:
         return MP_EINVAL;
     }
+    h->tune_gen++;
     return MP_OK;
 }

@@ -40,3 +40,28 @@ def test_tune_set_rejects_bad_values(eng):
         with pytest.raises(mp.MathpubError):
             eng.tune_set(**{knob: v})
     assert mp.lib().mp_tune_set(eng.handle, 99, 0) == mp.MP_EINVAL
+
+
+def test_graph_replay_after_other_heights_and_forms(eng):
+    """Batched calls replay a CUDA graph captured on an identical earlier call.  The graph
+    reads the scatter's CTA bounds from device memory, so a call at another height (other
+    bucket primes) or under another tuned form between two identical calls must not change
+    what the replay computes.  Plain-mode calls never use graphs and give the answer."""
+    import mathpub_b200 as mp
+    eng.tune_set(tile_log2=20, threads=1024, scatter_staged=1, bucket_div=1, no_pipeline=1)
+    ranges = [(10 ** 15, 10 ** 15 + (1 << 32)), (10 ** 12, 10 ** 12 + (1 << 32)), (10 ** 18, 10 ** 18 + (1 << 30))]
+    want = {}
+    for lo, hi in ranges:
+        r = eng.sieve_range(lo, hi, mode=mp.MODE_PLAIN)
+        want[lo] = {k: r[k] for k in KEYS}
+    seq = [0, 0, 1, 1, 0, 2, 2, 1, 0, 2]
+    for i in seq:
+        lo, hi = ranges[i]
+        r = eng.sieve_range(lo, hi)
+        assert {k: r[k] for k in KEYS} == want[lo], (i, lo)
+    # the same call under each form in turn, twice each (direct run, then replay)
+    for staged, div in [(1, 2), (0, 1), (1, 4), (1, 1)]:
+        eng.tune_set(scatter_staged=staged, bucket_div=div)
+        for _ in range(2):
+            r = eng.sieve_range(*ranges[0])
+            assert {k: r[k] for k in KEYS} == want[ranges[0][0]], (staged, div)
