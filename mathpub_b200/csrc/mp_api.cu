@@ -84,7 +84,7 @@ int mp_init(int device, mp_handle **out)
     }
     h->graphs = new GraphCache();
     DevBuf *bufs[] = {&h->tilesum, &h->blockacc, &h->rec, &h->reccnt, &h->queue, &h->errflag, &h->scratch_bitmap,
-                      &h->bpsw_n, &h->bpsw_bits, &h->ferm_p, &h->ferm_q, &h->ferm_part, &h->stats_out, &h->small_out,
+                      &h->bpsw_n, &h->bpsw_bits, &h->bpsw_list, &h->ferm_p, &h->ferm_q, &h->ferm_part, &h->stats_out, &h->small_out,
                       &h->boot.q, &h->boot.magic, &h->table.q, &h->table.magic, &h->tstate, &h->gap_acc};
     for (DevBuf *b : bufs) b->gen = &h->buf_gen;
     for (auto &e : h->scat) e.buf.gen = &h->buf_gen;
@@ -100,7 +100,7 @@ int mp_free(mp_handle *h)
     mp_graphs_free(h);
     mp_chain_free(h);
     DevBuf *bufs[] = {&h->tilesum, &h->blockacc, &h->rec, &h->reccnt, &h->queue, &h->errflag, &h->scratch_bitmap,
-                      &h->bpsw_n, &h->bpsw_bits, &h->ferm_p, &h->ferm_q, &h->ferm_part, &h->stats_out, &h->small_out,
+                      &h->bpsw_n, &h->bpsw_bits, &h->bpsw_list, &h->ferm_p, &h->ferm_q, &h->ferm_part, &h->stats_out, &h->small_out,
                       &h->boot.q, &h->boot.magic, &h->table.q, &h->table.magic, &h->tstate, &h->gap_acc};
     for (DevBuf *b : bufs) b->release();
     for (auto &e : h->scat) e.buf.release();

@@ -14,10 +14,14 @@
 //            device work queue, trial-divide them, and file the survivors in three size
 //            classes (below 2^62, [2^62, 2^63), above; mp_mont64.cuh runs a different product
 //            form for each).  Each class runs the base-2 test in batches of 32 that are uniform
-//            in kind and nearly so in exponent length, the
-//            passers are compacted with warp ballots, the Lucas test runs on them, and the
-//            warp writes the chunk's verdict words.  Warps never wait for one another.  The
-//            warps per CTA and candidates per chunk are picked by the autotuner.
+//            in kind and nearly so in exponent length, the passers are compacted with warp
+//            ballots and appended to the launch's Lucas list, and the warp writes the chunk's
+//            verdict words.  Warps never wait for one another.  A second launch then runs the
+//            Lucas test over the whole list, one passer per thread, and sets the bits of the
+//            primes.  (Run inside each chunk, the few dozen passers of a chunk left most lanes
+//            idle through the Lucas ladder, and the Lucas phase took half of the time for 4%
+//            of the candidates.)  The warps per CTA and candidates per chunk are picked by the
+//            autotuner.
 #include "mp_mont64.cuh"
 
 #define TD_N 30            // odd primes 3..127
@@ -62,7 +66,8 @@ __global__ void __launch_bounds__(256) bpsw_plain_kernel(const u64 *__restrict__
 
 template <int BPSW_WARPS, int BPSW_WCHUNK>
 __global__ void __launch_bounds__(BPSW_WARPS * 32) bpsw_batched_kernel(const u64 *__restrict__ n, u64 total,
-                                                                       u32 *__restrict__ bits, u32 *queue)
+                                                                       u32 *__restrict__ bits, u32 *queue,
+                                                                       u32 *__restrict__ lucas_list)
 {
     __shared__ u16 s_idx[BPSW_WARPS][BPSW_WCHUNK];   // survivors: < 2^62 from the front, >= 2^62 from the back
     __shared__ u16 s_pas[BPSW_WARPS][BPSW_WCHUNK];   // base-2 passers
@@ -132,18 +137,30 @@ __global__ void __launch_bounds__(BPSW_WARPS * 32) bpsw_batched_kernel(const u64
             np += __popc(m);
         }
         __syncwarp();
-        // 3. strong Lucas test on the base-2 passers
-        for (u32 base = 0; base < np; base += 32) {
-            const u32 k = base + lane;
-            if (k < np) {
-                const u32 i = pas[k];
-                if (lucas_u64(__ldg(nc + i))) atomicOr(&wb[i >> 5], 1u << (i & 31));
-            }
-        }
+        // 3. the base-2 passers go to the launch's Lucas list (queue[1] counts it), which
+        //    bpsw_lucas_kernel works through in full warps once every chunk is done: a chunk
+        //    has a few dozen passers, too few to keep a warp's lanes busy through the Lucas
+        //    ladder, and their Selfridge searches differ in length
+        u32 g = 0;
+        if (lane == 0 && np) g = atomicAdd(queue + 1, np);
+        g = __shfl_sync(0xffffffffu, g, 0);
+        for (u32 k = lane; k < np; k += 32) lucas_list[g + k] = (u32)(c0 + pas[k]);
         __syncwarp();
         const u32 nwords = (len + 31) / 32;
         for (u32 w = lane; w < nwords; w += 32) bits[(c0 >> 5) + w] = wb[w];
         __syncwarp();
+    }
+}
+
+// the strong Lucas test on the list of base-2 passers of a batched launch (indices into n, count
+// at *count), one candidate per thread; a prime's verdict bit is set in its word
+__global__ void __launch_bounds__(256) bpsw_lucas_kernel(const u64 *__restrict__ n, const u32 *__restrict__ list,
+                                                         const u32 *count, u32 *bits)
+{
+    const u32 cnt = *count;
+    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
+        const u32 idx = list[i];
+        if (lucas_u64(__ldg(n + idx))) atomicOr(bits + (idx >> 5), 1u << (idx & 31));
     }
 }
 
@@ -174,9 +191,11 @@ static int bpsw_consts(mp_handle *h)
     return MP_OK;
 }
 
-// one persistent launch: as many CTAs as fit on the device, no more than the chunks need
+// one persistent launch: as many CTAs as fit on the device, no more than the chunks need;
+// then the Lucas launch over the passers it listed
 template <int WARPS, int CHUNK>
-static cudaError_t bpsw_batched_launch(mp_handle *h, const u64 *d_n, u64 total, u32 *d_bits, cudaStream_t st)
+static cudaError_t bpsw_batched_launch(mp_handle *h, const u64 *d_n, u64 total, u32 *d_bits, u32 *d_list,
+                                       cudaStream_t st)
 {
     int per_sm = 0;
     cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bpsw_batched_kernel<WARPS, CHUNK>,
@@ -187,7 +206,18 @@ static cudaError_t bpsw_batched_launch(mp_handle *h, const u64 *d_n, u64 total, 
     const u64 nchunks = (total + CHUNK - 1) / CHUNK;
     const u64 need = (nchunks + WARPS - 1) / WARPS;
     if (grid > need) grid = need;
-    bpsw_batched_kernel<WARPS, CHUNK><<<(unsigned)grid, WARPS * 32, 0, st>>>(d_n, total, d_bits, h->queue.as<u32>());
+    u32 *queue = h->queue.as<u32>();
+    bpsw_batched_kernel<WARPS, CHUNK><<<(unsigned)grid, WARPS * 32, 0, st>>>(d_n, total, d_bits, queue, d_list);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    int lper = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&lper, bpsw_lucas_kernel, 256, 0);
+    if (e != cudaSuccess) return e;
+    if (lper < 1) lper = 1;
+    u64 lgrid = (u64)h->sm_count * lper;
+    const u64 lneed = (total + 255) / 256;
+    if (lgrid > lneed) lgrid = lneed;
+    bpsw_lucas_kernel<<<(unsigned)lgrid, 256, 0, st>>>(d_n, d_list, queue + 1, d_bits);
     return cudaGetLastError();
 }
 
@@ -209,14 +239,22 @@ int mp_bpsw_run(mp_handle *h, const u64 *d_n, const u64 *offs, const u32 *lens, 
     }
     const u64 total = offs[nlists];
     if (!total) return MP_OK;
+    // slices of at most 2^31 candidates, so that the Lucas list holds 32-bit indices
+    const u64 slice = 1ull << 31;
     MP_CUDA(h, h->queue.ensure(64));
-    MP_CUDA(h, cudaMemsetAsync(h->queue.p, 0, 4, st));
+    MP_CUDA(h, h->bpsw_list.ensure((size_t)std::min(total, slice) * 4));
     ProfScope ps(h, PROF_BPSW_BATCHED, st);
-    switch (h->tune.bpsw_variant) {
-    case 1: MP_CUDA(h, (bpsw_batched_launch<4, 1024>(h, d_n, total, d_bits, st))); break;
-    case 2: MP_CUDA(h, (bpsw_batched_launch<8, 512>(h, d_n, total, d_bits, st))); break;
-    case 3: MP_CUDA(h, (bpsw_batched_launch<16, 512>(h, d_n, total, d_bits, st))); break;
-    default: MP_CUDA(h, (bpsw_batched_launch<8, 1024>(h, d_n, total, d_bits, st))); break;
+    for (u64 b = 0; b < total; b += slice) {
+        const u64 t = std::min(slice, total - b);
+        const u64 *dn = d_n + b;
+        u32 *db = d_bits + b / 32, *dl = h->bpsw_list.as<u32>();
+        MP_CUDA(h, cudaMemsetAsync(h->queue.p, 0, 8, st));
+        switch (h->tune.bpsw_variant) {
+        case 1: MP_CUDA(h, (bpsw_batched_launch<4, 1024>(h, dn, t, db, dl, st))); break;
+        case 2: MP_CUDA(h, (bpsw_batched_launch<8, 512>(h, dn, t, db, dl, st))); break;
+        case 3: MP_CUDA(h, (bpsw_batched_launch<16, 512>(h, dn, t, db, dl, st))); break;
+        default: MP_CUDA(h, (bpsw_batched_launch<8, 1024>(h, dn, t, db, dl, st))); break;
+        }
     }
     return MP_OK;
 }

@@ -206,7 +206,7 @@ struct mp_handle {
     int servers_open = 0;            // servers sharing this handle's table (it may not be rebuilt)
 
     // scratch
-    DevBuf tilesum, blockacc, rec, reccnt, queue, errflag, scratch_bitmap, bpsw_n, bpsw_bits,
+    DevBuf tilesum, blockacc, rec, reccnt, queue, errflag, scratch_bitmap, bpsw_n, bpsw_bits, bpsw_list,
         ferm_p, ferm_q, ferm_part, stats_out, small_out, tstate, gap_acc;
     // CTA bounds of the bucket scatter, one buffer per (first prime, end prime, CTAs): a
     // captured graph reads the buffer it was captured with, so a buffer's contents are never

@@ -274,7 +274,13 @@ __device__ __forceinline__ void tile_run(const TileArgs &a, const Wave W, u32 rb
                 const u32 wi = __shfl_sync(0xffffffffu, w, i);
                 if (ji >= NB) continue;
                 const u32 j0 = ji + qi * (mp_w30_span(mp_w30_steps(wi), lane & 7) + 15u * (lane >> 3));
-                for (u32 j = j0; j < NB; j += 60u * qi) atomicOr(&sm[j >> 5], 1u << (j & 31));
+                const u32 d = 60u * qi;
+                u32 j = j0;
+                for (; j + d < NB; j += 2 * d) {
+                    atomicOr(&sm[j >> 5], __funnelshift_l(0u, 1u, j));
+                    atomicOr(&sm[(j + d) >> 5], __funnelshift_l(0u, 1u, j + d));
+                }
+                if (j < NB) atomicOr(&sm[j >> 5], __funnelshift_l(0u, 1u, j));
             }
         }
         // 3. thread tier, one thread per prime.  Dense primes (q < T / 32) have several
@@ -291,7 +297,12 @@ __device__ __forceinline__ void tile_run(const TileArgs &a, const Wave W, u32 rb
             const u32 turn = 15u * q;
 #pragma unroll
             for (int i = 0; i < 8; i++) {
-                for (u32 jj = j; jj < NB; jj += turn) atomicOr(&sm[jj >> 5], 1u << (jj & 31));
+                u32 jj = j;
+                for (; jj + turn < NB; jj += 2 * turn) {
+                    atomicOr(&sm[jj >> 5], __funnelshift_l(0u, 1u, jj));
+                    atomicOr(&sm[(jj + turn) >> 5], __funnelshift_l(0u, 1u, jj + turn));
+                }
+                if (jj < NB) atomicOr(&sm[jj >> 5], __funnelshift_l(0u, 1u, jj));
                 j += q * (s & 3u);
                 s >>= 2;
             }
@@ -328,10 +339,10 @@ __device__ __forceinline__ void tile_run(const TileArgs &a, const Wave W, u32 rb
                 }
                 u32 s = mp_w30_steps(w), n = 0;
                 for (; j < T; j += q * (s & 3u), s = __funnelshift_r(s, s, 2), n++)
-                    atomicOr(&sm[j >> 5], 1u << (j & 31));
+                    atomicOr(&sm[j >> 5], __funnelshift_l(0u, 1u, j));
                 if (keep) tst[kk - a.itd] = ((j - T) << 3) | ((w + n) & 7u);
                 for (; j < NB; j += q * (s & 3u), s = __funnelshift_r(s, s, 2))     // halo bits
-                    atomicOr(&sm[j >> 5], 1u << (j & 31));
+                    atomicOr(&sm[j >> 5], __funnelshift_l(0u, 1u, j));
             }
         }
         // 4. large primes: bucket records of this tile.  Records and bitmap words are read or
@@ -354,14 +365,14 @@ __device__ __forceinline__ void tile_run(const TileArgs &a, const Wave W, u32 rb
             }
             for (; i < n4; i += nth) {
                 const uint4 r0 = rec_ld(R4 + i, PIPE);
-                atomicOr(&sm[r0.x >> 5], 1u << (r0.x & 31));
-                atomicOr(&sm[r0.y >> 5], 1u << (r0.y & 31));
-                atomicOr(&sm[r0.z >> 5], 1u << (r0.z & 31));
-                atomicOr(&sm[r0.w >> 5], 1u << (r0.w & 31));
+                atomicOr(&sm[r0.x >> 5], __funnelshift_l(0u, 1u, r0.x));
+                atomicOr(&sm[r0.y >> 5], __funnelshift_l(0u, 1u, r0.y));
+                atomicOr(&sm[r0.z >> 5], __funnelshift_l(0u, 1u, r0.z));
+                atomicOr(&sm[r0.w >> 5], __funnelshift_l(0u, 1u, r0.w));
             }
             for (u32 k = (n4 << 2) + tid; k < n; k += nth) {
                 const u32 j = PIPE ? __ldcg(R + k) : __ldcs(R + k);
-                atomicOr(&sm[j >> 5], 1u << (j & 31));
+                atomicOr(&sm[j >> 5], __funnelshift_l(0u, 1u, j));
             }
         }
         __syncthreads();

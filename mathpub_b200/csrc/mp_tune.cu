@@ -119,10 +119,11 @@ extern "C" int mp_autotune(mp_handle *h, uint64_t lo, char *report, size_t cap)
     h->tune.fermat_variant = fv & 2;
     snprintf(line, sizeof line, "fermat choice: %d prime(s)/thread\n", (fv & 2) ? 2 : 1);
     rep += line;
-    // batched BPSW: 2^20 seeded odd candidates (three in four in [2^62, 2^64), the rest in
-    // [2^40, 2^62)), one list, each warps x chunk pair the kernel is built for
+    // batched BPSW: 2^23 seeded odd candidates (three in four in [2^62, 2^64), the rest in
+    // [2^40, 2^62)), one list, each warps x chunk pair the kernel is built for.  Enough chunks
+    // for several per warp: with fewer CTAs than SMs the launch's tail would decide
     {
-        const u64 cnt = 1ull << 20;
+        const u64 cnt = 1ull << 23;
         std::vector<u64> cand(cnt);
         u64 z = 0x5eed5eedull;
         for (u64 i = 0; i < cnt; i++) {
@@ -149,7 +150,7 @@ extern "C" int mp_autotune(mp_handle *h, uint64_t lo, char *report, size_t cap)
             MP_CUDA(h, cudaEventSynchronize(h->ev1));
             float ms = 0;
             MP_CUDA(h, cudaEventElapsedTime(&ms, h->ev0, h->ev1));
-            snprintf(line, sizeof line, "bpsw %s: %.3f ms for 2^20 candidates\n", mp_bpsw_variant_name(v), ms / 3);
+            snprintf(line, sizeof line, "bpsw %s: %.3f ms for 2^23 candidates\n", mp_bpsw_variant_name(v), ms / 3);
             rep += line;
             if (ms < bb) { bb = ms; bv = v; }
         }
