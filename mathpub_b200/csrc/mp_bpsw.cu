@@ -152,15 +152,31 @@ __global__ void __launch_bounds__(BPSW_WARPS * 32) bpsw_batched_kernel(const u64
     }
 }
 
-// the strong Lucas test on the list of base-2 passers of a batched launch (indices into n, count
-// at *count), one candidate per thread; a prime's verdict bit is set in its word
-__global__ void __launch_bounds__(256) bpsw_lucas_kernel(const u64 *__restrict__ n, const u32 *__restrict__ list,
-                                                         const u32 *count, u32 *bits)
+// The strong Lucas test on the list of base-2 passers of a batched launch (indices into n,
+// count at *count), one candidate per thread, in two launches: Selfridge's search for D, whose
+// length differs from candidate to candidate (a few Jacobi symbols, each after a 64-bit
+// remainder), stores D beside the index; then the Lucas ladder, the same length for every
+// candidate of a size, runs with the warps' lanes together, and a prime's verdict bit is set
+// in its word.  D = 0: shown composite by the search.
+__global__ void __launch_bounds__(256) bpsw_selfridge_kernel(const u64 *__restrict__ n, const u32 *__restrict__ list,
+                                                             const u32 *count, i32 *__restrict__ dlist)
 {
     const u32 cnt = *count;
     for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
+        const u64 x = __ldg(n + list[i]);
+        dlist[i] = x == ~0ull ? 0 : selfridge_d(x);                     // 3 | 2^64 - 1
+    }
+}
+
+__global__ void __launch_bounds__(256) bpsw_lucas_kernel(const u64 *__restrict__ n, const u32 *__restrict__ list,
+                                                         const i32 *__restrict__ dlist, const u32 *count, u32 *bits)
+{
+    const u32 cnt = *count;
+    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
+        const i32 D = dlist[i];
+        if (!D) continue;
         const u32 idx = list[i];
-        if (lucas_u64(__ldg(n + idx))) atomicOr(bits + (idx >> 5), 1u << (idx & 31));
+        if (lucas_strong(mm_setup(__ldg(n + idx)), D)) atomicOr(bits + (idx >> 5), 1u << (idx & 31));
     }
 }
 
@@ -195,7 +211,7 @@ static int bpsw_consts(mp_handle *h)
 // then the Lucas launch over the passers it listed
 template <int WARPS, int CHUNK>
 static cudaError_t bpsw_batched_launch(mp_handle *h, const u64 *d_n, u64 total, u32 *d_bits, u32 *d_list,
-                                       cudaStream_t st)
+                                       i32 *d_dlist, cudaStream_t st)
 {
     int per_sm = 0;
     cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bpsw_batched_kernel<WARPS, CHUNK>,
@@ -217,7 +233,8 @@ static cudaError_t bpsw_batched_launch(mp_handle *h, const u64 *d_n, u64 total, 
     u64 lgrid = (u64)h->sm_count * lper;
     const u64 lneed = (total + 255) / 256;
     if (lgrid > lneed) lgrid = lneed;
-    bpsw_lucas_kernel<<<(unsigned)lgrid, 256, 0, st>>>(d_n, d_list, queue + 1, d_bits);
+    bpsw_selfridge_kernel<<<(unsigned)lgrid, 256, 0, st>>>(d_n, d_list, queue + 1, d_dlist);
+    bpsw_lucas_kernel<<<(unsigned)lgrid, 256, 0, st>>>(d_n, d_list, d_dlist, queue + 1, d_bits);
     return cudaGetLastError();
 }
 
@@ -242,18 +259,20 @@ int mp_bpsw_run(mp_handle *h, const u64 *d_n, const u64 *offs, const u32 *lens, 
     // slices of at most 2^31 candidates, so that the Lucas list holds 32-bit indices
     const u64 slice = 1ull << 31;
     MP_CUDA(h, h->queue.ensure(64));
-    MP_CUDA(h, h->bpsw_list.ensure((size_t)std::min(total, slice) * 4));
+    const u64 lcap = std::min(total, slice);
+    MP_CUDA(h, h->bpsw_list.ensure((size_t)lcap * 8));          // indices, then the D of each
     ProfScope ps(h, PROF_BPSW_BATCHED, st);
     for (u64 b = 0; b < total; b += slice) {
         const u64 t = std::min(slice, total - b);
         const u64 *dn = d_n + b;
         u32 *db = d_bits + b / 32, *dl = h->bpsw_list.as<u32>();
+        i32 *dd = (i32 *)(dl + lcap);
         MP_CUDA(h, cudaMemsetAsync(h->queue.p, 0, 8, st));
         switch (h->tune.bpsw_variant) {
-        case 1: MP_CUDA(h, (bpsw_batched_launch<4, 1024>(h, dn, t, db, dl, st))); break;
-        case 2: MP_CUDA(h, (bpsw_batched_launch<8, 512>(h, dn, t, db, dl, st))); break;
-        case 3: MP_CUDA(h, (bpsw_batched_launch<16, 512>(h, dn, t, db, dl, st))); break;
-        default: MP_CUDA(h, (bpsw_batched_launch<8, 1024>(h, dn, t, db, dl, st))); break;
+        case 1: MP_CUDA(h, (bpsw_batched_launch<4, 1024>(h, dn, t, db, dl, dd, st))); break;
+        case 2: MP_CUDA(h, (bpsw_batched_launch<8, 512>(h, dn, t, db, dl, dd, st))); break;
+        case 3: MP_CUDA(h, (bpsw_batched_launch<16, 512>(h, dn, t, db, dl, dd, st))); break;
+        default: MP_CUDA(h, (bpsw_batched_launch<8, 1024>(h, dn, t, db, dl, dd, st))); break;
         }
     }
     return MP_OK;
