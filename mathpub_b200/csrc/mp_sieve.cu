@@ -31,7 +31,12 @@
 
 #define HALO_WORDS 32u
 #define HALO_BITS (HALO_WORDS * 32u)
-#define QWARP 2048u
+// tier bounds: the warp tier takes 97 <= q < QWARP, the dense thread tier QWARP <= q < QDENSE
+// (never above T / 32), the sparse thread tier the rest up to the bucket threshold.  Measured
+// at config 2 (2^20-bit tiles): QWARP 4096 and QDENSE 8192 (T / 128) 5.95 ms of tile kernel,
+// 2048 and T / 32 6.05 ms, 8192 and T / 32 6.10 ms, 2048 and T / 16 6.14 ms
+#define QWARP 4096u
+#define QDENSE 8192u
 #define PAT_MAXQ 89u
 #define MAX_TLOG 20
 
@@ -283,7 +288,7 @@ __device__ __forceinline__ void tile_run(const TileArgs &a, const Wave W, u32 rb
                 if (j < NB) atomicOr(&sm[j >> 5], __funnelshift_l(0u, 1u, j));
             }
         }
-        // 3. thread tier, one thread per prime.  Dense primes (q < T / 32) have several
+        // 3. thread tier, one thread per prime.  Dense primes (q < QDENSE) have several
         //    multiples per residue of the wheel in a tile: set up from x0 in every tile and
         //    walked as 8 progressions of stride 15 q.
         for (u32 k = a.iw1 + tid; k < a.itd; k += nth) {
@@ -307,7 +312,7 @@ __device__ __forceinline__ void tile_run(const TileArgs &a, const Wave W, u32 rb
                 s >>= 2;
             }
         }
-        //    Sparse primes (T / 32 <= q <= T) have a few multiples per tile: one walk through
+        //    Sparse primes (QDENSE <= q <= T) have a few multiples per tile: one walk through
         //    the residues, with the next multiple carried to the CTA's next tile, so that the
         //    modular set-up runs once per run of tiles.  Four primes per thread are loaded
         //    ahead.
@@ -1350,7 +1355,7 @@ static Tiers tiers_for(const PrimeTable &tb, u32 tlog, u64 top, u64 qbucket)
     r.iw0 = (u32)std::min<u64>(tb.count_le(PAT_MAXQ), r.iend);
     r.iw1 = (u32)std::min<u64>(tb.count_le(QWARP - 1), r.iend);
     r.it1 = (u32)std::min<u64>(tb.count_le(qbucket), r.iend);
-    r.itd = std::max(r.iw1, (u32)std::min<u64>(tb.count_le((1ull << tlog) / 32 - 1), r.it1));
+    r.itd = std::max(r.iw1, (u32)std::min<u64>(tb.count_le(std::min<u64>(QDENSE, (1ull << tlog) / 32) - 1), r.it1));
     return r;
 }
 
