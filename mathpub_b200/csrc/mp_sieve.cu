@@ -314,18 +314,18 @@ __device__ __forceinline__ void tile_run(const TileArgs &a, const Wave W, u32 rb
         }
         //    Sparse primes (QDENSE <= q <= T) have a few multiples per tile: one walk through
         //    the residues, with the next multiple carried to the CTA's next tile, so that the
-        //    modular set-up runs once per run of tiles.  Four primes per thread are loaded
+        //    modular set-up runs once per run of tiles.  Eight primes per thread are loaded
         //    ahead.
-        for (u32 k = a.itd + tid; k < a.it1; k += 4 * nth) {
-            u32 qv[4], sv[4];
+        for (u32 k = a.itd + tid; k < a.it1; k += 8 * nth) {
+            u32 qv[8], sv[8];
 #pragma unroll
-            for (int u = 0; u < 4; u++) {
+            for (int u = 0; u < 8; u++) {
                 const u32 kk = k + u * nth;
                 qv[u] = kk < a.it1 ? __ldg(a.q + kk) : 0u;
                 sv[u] = (kk < a.it1 && !fresh) ? tst[kk - a.itd] : W30_NOSTATE;
             }
 #pragma unroll
-            for (int u = 0; u < 4; u++) {
+            for (int u = 0; u < 8; u++) {
                 const u32 q = qv[u];
                 if (!q) continue;
                 const u32 kk = k + u * nth;
