@@ -1359,22 +1359,44 @@ static Tiers tiers_for(const PrimeTable &tb, u32 tlog, u64 top, u64 qbucket)
     return r;
 }
 
+// the tile kernel's dynamic shared memory, with its limit raised once per device
+template <int TLOG, int EMIT>
+static cudaError_t tile_smem(size_t *smem)
+{
+    *smem = ((1u << TLOG) / 32 + HALO_WORDS) * 4;
+    static bool attr_set[16] = {false};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 16) return cudaErrorInvalidDevice;
+    if (!attr_set[dev]) {
+        e = cudaFuncSetAttribute(tile_kernel<TLOG, EMIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem);
+        if (e != cudaSuccess) return e;
+        attr_set[dev] = true;
+    }
+    return cudaSuccess;
+}
+
 template <int TLOG, int EMIT>
 static cudaError_t launch_tile(const TileArgs &a, int grid, int nth, cudaStream_t st)
 {
-    const size_t smem = ((1u << TLOG) / 32 + HALO_WORDS) * 4;
-    static bool attr_set[16][64] = {{false}};
-    int dev = 0;
-    cudaGetDevice(&dev);
-    const int key = TLOG * 2 + EMIT;
-    if (dev < 0 || dev >= 16) return cudaErrorInvalidDevice;
-    if (!attr_set[dev][key]) {
-        cudaError_t e = cudaFuncSetAttribute(tile_kernel<TLOG, EMIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        attr_set[dev][key] = true;
-    }
+    size_t smem = 0;
+    const cudaError_t e = tile_smem<TLOG, EMIT>(&smem);
+    if (e != cudaSuccess) return e;
     tile_kernel<TLOG, EMIT><<<grid, nth, smem, st>>>(a);
     return cudaGetLastError();
+}
+
+// resident tile-kernel CTAs per SM at this geometry, from the occupancy calculation (shared
+// memory, threads and registers: at 64 registers a thread, 2048 threads of a 2^19-bit tile do
+// not fit on one SM although their shared memory does)
+template <int TLOG, int EMIT>
+static cudaError_t tile_occupancy(int nth, int *per_sm)
+{
+    size_t smem = 0;
+    const cudaError_t e = tile_smem<TLOG, EMIT>(&smem);
+    if (e != cudaSuccess) return e;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, tile_kernel<TLOG, EMIT>, nth, smem);
 }
 
 static cudaError_t launch_tile_any(const TileArgs &a, int grid, int nth, int emit, cudaStream_t st)
@@ -1390,13 +1412,23 @@ static cudaError_t launch_tile_any(const TileArgs &a, int grid, int nth, int emi
     }
 }
 
-// resident CTAs per SM for the tile kernel at this geometry
-static int tile_ctas_per_sm(u32 tlog, int nth)
+// resident CTAs per SM for the tile kernel at this geometry (at least 1)
+static int tile_ctas_per_sm(u32 tlog, int nth, int emit)
 {
-    const size_t smem = ((1u << tlog) / 32 + HALO_WORDS) * 4 + 2048;
-    int by_smem = (int)((227 * 1024) / smem);
-    int by_thr = 2048 / nth;
-    int r = std::min(by_smem, by_thr);
+    int r = 0;
+    cudaError_t e;
+    switch (tlog * 2 + (emit ? 1 : 0)) {
+    case 36: e = tile_occupancy<18, 0>(nth, &r); break;
+    case 37: e = tile_occupancy<18, 1>(nth, &r); break;
+    case 38: e = tile_occupancy<19, 0>(nth, &r); break;
+    case 39: e = tile_occupancy<19, 1>(nth, &r); break;
+    case 40: e = tile_occupancy<20, 0>(nth, &r); break;
+    default: e = tile_occupancy<20, 1>(nth, &r); break;
+    }
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        r = 1;
+    }
     return r < 1 ? 1 : r;
 }
 
@@ -1666,7 +1698,7 @@ static int run_tiles(mp_handle *h, const PrimeTable &tb, const SievePlan &P, Til
     const int nth = P.nth;
     const u32 plain_w = (u32)std::max(1, h->sm_count);
     const u32 nlaunch = mode == 1 ? (P.g.ntiles + plain_w - 1) / plain_w : P.nwaves;
-    const int grid_pers = h->sm_count * tile_ctas_per_sm(P.g.tlog, nth);
+    const int grid_pers = h->sm_count * tile_ctas_per_sm(P.g.tlog, nth, emit);
     // carried state of the sparse thread-tier primes: one slot per prime per CTA (written and
     // read by the tile kernel only; nothing needs clearing)
     MP_CUDA(h, h->tstate.ensure((size_t)grid_pers * (P.ti.it1 - P.ti.itd) * 4 + 64));
