@@ -91,7 +91,9 @@ typedef mp_range_stats mp_block_stats;
 /* MP_MODE_BATCHED: the range in waves of tiles; per wave a bucket scatter for the large
  *   primes, then a tile launch in which each CTA sieves a contiguous run of tiles and carries
  *   the state of its sparse primes from tile to tile; the whole call is captured once as a
- *   CUDA graph and replayed.
+ *   CUDA graph and replayed.  With the binned scatter (mp_tune_set) and no
+ *   MP_TUNE_NO_PIPELINE, one persistent launch runs every wave's scatter and tile work from a
+ *   device queue instead.
  * MP_MODE_PLAIN: the reference's per-segment launch loop on a full grid: one launch per group
  *   of SM-count 32 KiB segments, one segment per CTA, every segment set up from scratch,
  *   each group with its own bucket scatter; no graph. */
@@ -234,8 +236,9 @@ int mp_bpsw_batches(mp_handle *h, const uint64_t *const *lists, const uint32_t *
 
 /* device form: candidates laid out as nlists lists, list i at d_n + offs[i] (offs[i] a
    multiple of 32, host array offs[0..nlists]), verdict words (u32, bit i & 31 of word
-   i >> 5) at d_bits + offs[i] / 32; mode MP_MODE_BATCHED (one persistent launch) or
-   MP_MODE_PLAIN (one launch per list) */
+   i >> 5) at d_bits + offs[i] / 32; mode MP_MODE_BATCHED (one persistent launch over
+   every list for trial division and the base-2 test, then two launches for the Lucas test
+   on the base-2 passers) or MP_MODE_PLAIN (one launch per list) */
 int mp_bpsw_lists_dev(mp_handle *h, const uint64_t *d_n, const uint64_t *offs,
                       const uint32_t *lens, uint32_t nlists, uint32_t *d_bits, uint32_t mode,
                       void *stream);
@@ -299,7 +302,8 @@ int mp_autotune(mp_handle *h, uint64_t lo, char *report, size_t cap);
  *   MP_TUNE_SCATTER_STAGED 1: the staged bucket scatter, 0: the binned one
  *   MP_TUNE_BUCKET_DIV     primes above tile bits / value (1, 2 or 4) go to the buckets
  *   MP_TUNE_NO_PIPELINE    1: batched sieve calls as a host loop of wave launches, 0: one
- *                          persistent pipeline launch
+ *                          persistent pipeline launch (with the binned scatter only; the
+ *                          staged scatter always runs the wave loop)
  *   MP_TUNE_BPSW_VARIANT   0..3: warps x candidates per chunk of the batched BPSW kernel
  *   MP_TUNE_FERMAT_ILP2    1: two primes per thread in the Fermat kernel
  * Returns MP_EINVAL for an unknown knob or a value out of range.  No reference counterpart
