@@ -16,12 +16,13 @@
 //            form for each).  Each class runs the base-2 test in batches of 32 that are uniform
 //            in kind and nearly so in exponent length, the passers are compacted with warp
 //            ballots and appended to the launch's Lucas list, and the warp writes the chunk's
-//            verdict words.  Warps never wait for one another.  A second launch then runs the
-//            Lucas test over the whole list, one passer per thread, and sets the bits of the
-//            primes.  (Run inside each chunk, the few dozen passers of a chunk left most lanes
-//            idle through the Lucas ladder, and the Lucas phase took half of the time for 4%
-//            of the candidates.)  The warps per CTA and candidates per chunk are picked by the
-//            autotuner.
+//            verdict words.  Warps never wait for one another.  Two more launches then run
+//            the Lucas test over the whole list, one passer per thread: Selfridge's search
+//            files the passers by D (D = 5 apart), and the ladders set the bits of the primes,
+//            those with D = 5 in a two-product step.  (Run inside each chunk, the few dozen
+//            passers of a chunk left most lanes idle through the Lucas ladder, and the Lucas
+//            phase took half of the time for 4% of the candidates.)  The warps per CTA and
+//            candidates per chunk are picked by the autotuner.
 #include "mp_mont64.cuh"
 
 #define TD_N 30            // odd primes 3..127
@@ -153,30 +154,55 @@ __global__ void __launch_bounds__(BPSW_WARPS * 32) bpsw_batched_kernel(const u64
 }
 
 // The strong Lucas test on the list of base-2 passers of a batched launch (indices into n,
-// count at *count), one candidate per thread, in two launches: Selfridge's search for D, whose
+// count at *count), one candidate per thread, in two launches.  Selfridge's search for D, whose
 // length differs from candidate to candidate (a few Jacobi symbols, each after a 64-bit
-// remainder), stores D beside the index; then the Lucas ladder, the same length for every
-// candidate of a size, runs with the warps' lanes together, and a prime's verdict bit is set
-// in its word.  D = 0: shown composite by the search.
+// remainder), files each candidate: D = 5 (about half of them: n = 2 or 3 mod 5) in one list,
+// any other D with its value in another; D = 0 (shown composite by the search) in neither.
+// Then the Lucas ladders run with the warps' lanes together, the D = 5 list first with its
+// two-product step (Q = -1), and a prime's verdict bit is set in its word.  Lists: l5 indices
+// (count ctr[0]); lo indices and dl their D (count ctr[1]).
 __global__ void __launch_bounds__(256) bpsw_selfridge_kernel(const u64 *__restrict__ n, const u32 *__restrict__ list,
-                                                             const u32 *count, i32 *__restrict__ dlist)
+                                                             const u32 *count, u32 *__restrict__ l5,
+                                                             u32 *__restrict__ lo, i32 *__restrict__ dl, u32 *ctr)
 {
-    const u32 cnt = *count;
-    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
-        const u64 x = __ldg(n + list[i]);
-        dlist[i] = x == ~0ull ? 0 : selfridge_d(x);                     // 3 | 2^64 - 1
+    const u32 cnt = *count, lane = threadIdx.x & 31, lt = (1u << lane) - 1;
+    // warp-uniform trip count, so that every lane takes part in the ballots
+    for (u32 b0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); b0 < cnt; b0 += gridDim.x * blockDim.x) {
+        const u32 i = b0 + lane;
+        u32 idx = 0;
+        i32 D = 0;
+        if (i < cnt) {
+            idx = list[i];
+            const u64 x = __ldg(n + idx);
+            D = x == ~0ull ? 0 : selfridge_d(x);                         // 3 | 2^64 - 1
+        }
+        const u32 m5 = __ballot_sync(0xffffffffu, D == 5), mo = __ballot_sync(0xffffffffu, D != 0 && D != 5);
+        u32 g5 = 0, go = 0;
+        if (lane == 0) {
+            if (m5) g5 = atomicAdd(ctr, (u32)__popc(m5));
+            if (mo) go = atomicAdd(ctr + 1, (u32)__popc(mo));
+        }
+        g5 = __shfl_sync(0xffffffffu, g5, 0);
+        go = __shfl_sync(0xffffffffu, go, 0);
+        if (D == 5) l5[g5 + __popc(m5 & lt)] = idx;
+        else if (D) {
+            const u32 k = go + __popc(mo & lt);
+            lo[k] = idx;
+            dl[k] = D;
+        }
     }
 }
 
-__global__ void __launch_bounds__(256) bpsw_lucas_kernel(const u64 *__restrict__ n, const u32 *__restrict__ list,
-                                                         const i32 *__restrict__ dlist, const u32 *count, u32 *bits)
+__global__ void __launch_bounds__(256) bpsw_lucas_kernel(const u64 *__restrict__ n, const u32 *__restrict__ l5,
+                                                         const u32 *__restrict__ lo, const i32 *__restrict__ dl,
+                                                         const u32 *ctr, u32 *bits)
 {
-    const u32 cnt = *count;
+    const u32 c5 = ctr[0], cnt = c5 + ctr[1];
     for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
-        const i32 D = dlist[i];
-        if (!D) continue;
-        const u32 idx = list[i];
-        if (lucas_strong(mm_setup(__ldg(n + idx)), D)) atomicOr(bits + (idx >> 5), 1u << (idx & 31));
+        const bool f = i < c5;
+        const u32 idx = f ? l5[i] : lo[i - c5];
+        const Mod64 M = mm_setup(__ldg(n + idx));
+        if (f ? lucas_strong_d5(M) : lucas_strong(M, dl[i - c5])) atomicOr(bits + (idx >> 5), 1u << (idx & 31));
     }
 }
 
@@ -211,7 +237,7 @@ static int bpsw_consts(mp_handle *h)
 // then the Lucas launch over the passers it listed
 template <int WARPS, int CHUNK>
 static cudaError_t bpsw_batched_launch(mp_handle *h, const u64 *d_n, u64 total, u32 *d_bits, u32 *d_list,
-                                       i32 *d_dlist, cudaStream_t st)
+                                       u64 lcap, cudaStream_t st)
 {
     int per_sm = 0;
     cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bpsw_batched_kernel<WARPS, CHUNK>,
@@ -233,8 +259,10 @@ static cudaError_t bpsw_batched_launch(mp_handle *h, const u64 *d_n, u64 total, 
     u64 lgrid = (u64)h->sm_count * lper;
     const u64 lneed = (total + 255) / 256;
     if (lgrid > lneed) lgrid = lneed;
-    bpsw_selfridge_kernel<<<(unsigned)lgrid, 256, 0, st>>>(d_n, d_list, queue + 1, d_dlist);
-    bpsw_lucas_kernel<<<(unsigned)lgrid, 256, 0, st>>>(d_n, d_list, d_dlist, queue + 1, d_bits);
+    u32 *l5 = d_list + lcap, *lo = d_list + 2 * lcap;
+    i32 *dl = (i32 *)(d_list + 3 * lcap);
+    bpsw_selfridge_kernel<<<(unsigned)lgrid, 256, 0, st>>>(d_n, d_list, queue + 1, l5, lo, dl, queue + 2);
+    bpsw_lucas_kernel<<<(unsigned)lgrid, 256, 0, st>>>(d_n, l5, lo, dl, queue + 2, d_bits);
     return cudaGetLastError();
 }
 
@@ -260,19 +288,18 @@ int mp_bpsw_run(mp_handle *h, const u64 *d_n, const u64 *offs, const u32 *lens, 
     const u64 slice = 1ull << 31;
     MP_CUDA(h, h->queue.ensure(64));
     const u64 lcap = std::min(total, slice);
-    MP_CUDA(h, h->bpsw_list.ensure((size_t)lcap * 8));          // indices, then the D of each
+    MP_CUDA(h, h->bpsw_list.ensure((size_t)lcap * 16));         // passers; D = 5 ones; others; their D
     ProfScope ps(h, PROF_BPSW_BATCHED, st);
     for (u64 b = 0; b < total; b += slice) {
         const u64 t = std::min(slice, total - b);
         const u64 *dn = d_n + b;
         u32 *db = d_bits + b / 32, *dl = h->bpsw_list.as<u32>();
-        i32 *dd = (i32 *)(dl + lcap);
-        MP_CUDA(h, cudaMemsetAsync(h->queue.p, 0, 8, st));
+        MP_CUDA(h, cudaMemsetAsync(h->queue.p, 0, 16, st));
         switch (h->tune.bpsw_variant) {
-        case 1: MP_CUDA(h, (bpsw_batched_launch<4, 1024>(h, dn, t, db, dl, dd, st))); break;
-        case 2: MP_CUDA(h, (bpsw_batched_launch<8, 512>(h, dn, t, db, dl, dd, st))); break;
-        case 3: MP_CUDA(h, (bpsw_batched_launch<16, 512>(h, dn, t, db, dl, dd, st))); break;
-        default: MP_CUDA(h, (bpsw_batched_launch<8, 1024>(h, dn, t, db, dl, dd, st))); break;
+        case 1: MP_CUDA(h, (bpsw_batched_launch<4, 1024>(h, dn, t, db, dl, lcap, st))); break;
+        case 2: MP_CUDA(h, (bpsw_batched_launch<8, 512>(h, dn, t, db, dl, lcap, st))); break;
+        case 3: MP_CUDA(h, (bpsw_batched_launch<16, 512>(h, dn, t, db, dl, lcap, st))); break;
+        default: MP_CUDA(h, (bpsw_batched_launch<8, 1024>(h, dn, t, db, dl, lcap, st))); break;
         }
     }
     return MP_OK;

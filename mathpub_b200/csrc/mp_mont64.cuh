@@ -405,6 +405,41 @@ __device__ __forceinline__ bool lucas_strong(const Mod64 &M, i32 D)
     return false;
 }
 
+// the same test for D = 5 (P = 1, Q = -1), the D of about half of all candidates: Q^k = (-1)^k is
+// a sign, so a ladder step takes the two V products only.  From (V_k, V_k+1) with Q^k = sg:
+// V_2k+1 = V_k V_k+1 - sg, V_2k = V_k^2 - 2 sg, V_2k+2 = V_k+1^2 + 2 sg (Q^(k+1) = -sg); k's
+// parity after the step is the exponent bit.  Then Q^d = -1 (d odd), so V_2d = V_d^2 + 2 and
+// V_(d 2^r) = V^2 - 2 for r >= 2.
+__device__ __forceinline__ bool lucas_strong_d5(const Mod64 &M)
+{
+    const u64 n = M.n;
+    const int s = __ffsll((long long)(n + 1)) - 1;
+    const u64 d = (n + 1) >> s;
+    const u64 one = M.one, two = mm_add(one, one, n);
+    // k = 1: V_1 = 1, V_2 = 1 + 2 = 3, Q^1 = -1
+    u64 vk = one, vk1 = mm_add(two, one, n);
+    bool neg = true;                                                   // Q^k = -1
+    for (int i = 62 - __clzll((long long)d); i >= 0; i--) {
+        const bool b = (d >> i) & 1;
+        const u64 p = ms_mul(vk, vk1, M);
+        const u64 w = neg ? mm_add(p, one, n) : mm_sub(p, one, n);     // V_2k+1
+        const u64 sq = ms_sqr(b ? vk1 : vk, M);
+        // V_2k = sq - 2 sg; V_2k+2 = sq + 2 sg: subtract 2 exactly when (sg = +1) != b
+        const bool sub2 = (!neg) != b;
+        const u64 v2 = sub2 ? mm_sub(sq, two, n) : mm_add(sq, two, n);
+        vk = b ? w : v2;
+        vk1 = b ? v2 : w;
+        neg = b;
+    }
+    if (vk == 0 || mm_add(vk1, vk1, n) == vk) return true;             // V_d = 0 or U_d = 0
+    for (int r = 1; r < s; r++) {
+        const u64 sq = ms_sqr(vk, M);
+        vk = r == 1 ? mm_add(sq, two, n) : mm_sub(sq, two, n);         // V_(d 2^r)
+        if (vk == 0) return true;
+    }
+    return false;
+}
+
 // the Lucas half of BPSW for an odd n > 2 that passed the base-2 test
 __device__ __forceinline__ bool lucas_u64(u64 n)
 {
