@@ -44,7 +44,7 @@ BPSW_SEED, BPSW_COUNT, BPSW_LISTS = 0x3C0FFEE, 1 << 26, 4096
 HBM_FALLBACK_GBS = 6650.0
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one tile-kernel launch (a wave
 # of 1184 tiles at 1e15), from an ncu capture of that launch
-TILE_TRAFFIC_BYTES = 597.8e6 + 293.2e6
+TILE_TRAFFIC_BYTES = 597.9e6 + 297.7e6
 # the same for the persistent pipeline launch of one step (None until captured)
 PIPE_TRAFFIC_BYTES = None
 WORKLOAD = ("large-offset sieve [1e15, 1e15+2^34) per GPU, odd-only bitmap, sieving primes up to 31623048, "
@@ -155,9 +155,10 @@ IMAD_PER_PRODUCT_FERMAT_K3 = 39
 def bpsw_products(n, prime_mask):
     """Montgomery products of the BPSW kernels on the candidates n, counted exactly from the
     inputs: the base-2 ladder of every candidate that trial division leaves (bitlen(d) - 1
-    squarings, n - 1 = d 2^s) and the Lucas ladder of every prime among them (four products per
-    step, bitlen(d') - 1 steps, n + 1 = d' 2^s').  The squarings of the strong chains after the
-    ladders and the set-up are left out, so this is a lower bound on the work."""
+    squarings, n - 1 = d 2^s) and the Lucas ladder of every prime among them (bitlen(d') - 1
+    steps, n + 1 = d' 2^s'; two products a step where Selfridge's D is 5, that is n = 2 or 3
+    mod 5, four otherwise).  The squarings of the strong chains after the ladders and the set-up
+    are left out, so this is a lower bound on the work."""
     n = np.asarray(n, dtype=np.uint64)
     surv = ((n & np.uint64(1)) == 1) & (n >= np.uint64(131 * 131))
     for q in TD_PRIMES:
@@ -166,7 +167,10 @@ def bpsw_products(n, prime_mask):
     sprp = int((_bitlen64(_odd_part(ns - np.uint64(1))) - 1).sum())
     npr = n[surv & prime_mask]
     npr = npr[npr != np.uint64(0xffffffffffffffff)]
-    lucas = 4 * int((_bitlen64(_odd_part(npr + np.uint64(1))) - 1).sum())
+    steps = _bitlen64(_odd_part(npr + np.uint64(1))) - 1
+    m5 = npr % np.uint64(5)
+    per = np.where((m5 == 2) | (m5 == 3), 2, 4)
+    lucas = int((per * steps).sum())
     return sprp, lucas, int(surv.sum()), int(len(npr))
 
 
