@@ -11,10 +11,10 @@
 // Two launch structures:
 //   plain    one launch per candidate list, one thread per candidate, all phases inline;
 //   batched  one persistent launch over every list: warps pop chunks of candidates from a
-//            device work queue, trial-divide them, and file the survivors in three size
-//            classes (below 2^62, [2^62, 2^63), above; mp_mont64.cuh runs a different product
-//            form for each).  Each class runs the base-2 test in batches of 32 that are uniform
-//            in kind and nearly so in exponent length, the passers are compacted with warp
+//            device work queue, trial-divide them, and file the survivors in two size classes
+//            (below 2^63 and above; mp_mont64.cuh runs a different ladder step for each).
+//            Each class runs the base-2 test in batches of 32 that are uniform in kind and
+//            nearly so in exponent length, the passers are compacted with warp
 //            ballots and appended to the launch's Lucas list, and the warp writes the chunk's
 //            verdict words.  Warps never wait for one another.  Two more launches then run
 //            the Lucas test over the whole list, one passer per thread: Selfridge's search
@@ -63,14 +63,13 @@ __global__ void __launch_bounds__(256) bpsw_plain_kernel(const u64 *__restrict__
 // ---- batched form: persistent warps over chunks of the concatenated lists ----
 // a work-queue chunk is BPSW_WCHUNK candidates per warp, BPSW_WARPS warps per CTA; the
 // autotuner picks among the instantiated pairs (bpsw_batched_launch)
-#define BPSW_LAZY_MAX (1ull << 62)
 
 template <int BPSW_WARPS, int BPSW_WCHUNK>
 __global__ void __launch_bounds__(BPSW_WARPS * 32) bpsw_batched_kernel(const u64 *__restrict__ n, u64 total,
                                                                        u32 *__restrict__ bits, u32 *queue,
                                                                        u32 *__restrict__ lucas_list)
 {
-    __shared__ u16 s_idx[BPSW_WARPS][BPSW_WCHUNK];   // survivors: < 2^62 from the front, >= 2^62 from the back
+    __shared__ u16 s_idx[BPSW_WARPS][BPSW_WCHUNK];   // survivors below 2^63
     __shared__ u16 s_pas[BPSW_WARPS][BPSW_WCHUNK];   // base-2 passers
     __shared__ u32 s_bits[BPSW_WARPS][BPSW_WCHUNK / 32];
     const u32 lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -87,23 +86,20 @@ __global__ void __launch_bounds__(BPSW_WARPS * 32) bpsw_batched_kernel(const u64
         const u32 len = (u32)(total - c0 < BPSW_WCHUNK ? total - c0 : BPSW_WCHUNK);
         const u64 *nc = n + c0;
         // 1. trial division: verdict words of the decided candidates; survivors filed by size
-        //    class: below 2^62 at the front of idx, [2^62, 2^63) at its back, 2^63 and above at
-        //    the front of pas (free until the base-2 passers are collected)
-        u32 ns = 0, nm = 0, nw = 0;
+        //    class: below 2^63 in idx, 2^63 and above in pas (free until the base-2 passers are
+        //    collected)
+        u32 nm = 0, nw = 0;
         for (u32 base = 0; base < len; base += 32) {
             const u32 i = base + lane;
             const u64 x = i < len ? __ldg(nc + i) : 0;
             const int v = i < len ? td_verdict(x) : 0;
             const u32 pm = __ballot_sync(0xffffffffu, v == 1);
             const int c = spsp2_class(x);
-            const bool cs = v < 0 && c == SP_LAZY, cm = v < 0 && c == SP_FOLD, cw = v < 0 && c == SP_WIDE;
-            const u32 ms = __ballot_sync(0xffffffffu, cs), mm = __ballot_sync(0xffffffffu, cm);
-            const u32 mw = __ballot_sync(0xffffffffu, cw);
+            const bool cm = v < 0 && c == SP_FOLD, cw = v < 0 && c == SP_WIDE;
+            const u32 mm = __ballot_sync(0xffffffffu, cm), mw = __ballot_sync(0xffffffffu, cw);
             if (lane == 0) wb[base >> 5] = pm;
-            if (cs) idx[ns + __popc(ms & lt)] = (u16)i;
-            if (cm) idx[BPSW_WCHUNK - 1 - (nm + __popc(mm & lt))] = (u16)i;
+            if (cm) idx[nm + __popc(mm & lt)] = (u16)i;
             if (cw) pas[nw + __popc(mw & lt)] = (u16)i;
-            ns += __popc(ms);
             nm += __popc(mm);
             nw += __popc(mw);
         }
@@ -123,16 +119,8 @@ __global__ void __launch_bounds__(BPSW_WARPS * 32) bpsw_batched_kernel(const u64
         }
         for (u32 base = 0; base < nm; base += 32) {
             const u32 k = base + lane;
-            const u32 i = k < nm ? idx[BPSW_WCHUNK - 1 - k] : 0;
+            const u32 i = k < nm ? idx[k] : 0;
             const bool pass = k < nm && spsp2<SP_FOLD>(mm_setup(__ldg(nc + i)));
-            const u32 m = __ballot_sync(0xffffffffu, pass);
-            if (pass) pas[np + __popc(m & lt)] = (u16)i;
-            np += __popc(m);
-        }
-        for (u32 base = 0; base < ns; base += 32) {
-            const u32 k = base + lane;
-            const u32 i = k < ns ? idx[k] : 0;
-            const bool pass = k < ns && spsp2<SP_LAZY>(mm_setup(__ldg(nc + i)));
             const u32 m = __ballot_sync(0xffffffffu, pass);
             if (pass) pas[np + __popc(m & lt)] = (u16)i;
             np += __popc(m);

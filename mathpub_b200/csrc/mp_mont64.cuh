@@ -9,18 +9,16 @@
 // this file's own design, from the published mathematics:
 //
 //  * A residue is two 32-bit limbs; each product is one PTX block of 32-bit multiply-add carry
-//    chains.  Two reductions of the 128-bit product t (R = 2^64):
-//      - adding: word by word, m = t_i (-n^-1) mod 2^32, t += m n 2^(32 i).  For n < 2^62 (so
-//        4n <= R) residues stay in [0, 2n) with no subtraction after a product (lazy);
-//      - subtracting: m = t n^-1 mod 2^64, then (t - m n) / R = t_hi - hi(m n), exact since the
-//        low halves agree, plus n when it borrows.  In and out in [0, n), for any odd n; fewer
-//        carry adds than the adding form, and its input may be up to n R, which lets the
-//        doubling below fold into the product for n < 2^63.
-//  * Base-2 exponentiation, left to right, in three size classes (warps run one class at a
-//    time): n < 2^62, lazy adding products, then a doubling by a funnel shift of the residue by
-//    the exponent bit b and one conditional subtraction (no select between two residues);
-//    2^62 <= n < 2^63, one subtracting product x (x 2^b) per bit (below 2 n^2 < n R);
-//    n >= 2^63, a subtracting square, then the doubling.
+//    chains, with the subtracting reduction of the 128-bit product t (R = 2^64): m = t n^-1 mod
+//    2^64, then (t - m n) / R = t_hi - hi(m n), exact since the low halves agree, plus n when it
+//    borrows.  In and out in [0, n), for any odd n, and its input may be up to n R, which lets
+//    the doubling below fold into the product for n < 2^63.
+//  * Base-2 exponentiation, left to right, in two size classes (warps run one class at a time):
+//    n < 2^63, one product x (x 2^b) per bit (below 2 n^2 < n R); n >= 2^63, a square, then a
+//    doubling by a funnel shift of the residue by the exponent bit b and one conditional
+//    subtraction (no select between two residues).  (A word-by-word adding reduction with lazy
+//    residues in [0, 2n) for n < 2^62, a square then a doubling per bit, measured 2.5% slower on
+//    the whole batched BPSW than the folded product.)
 //  * Lucas sequences (P = 1, Q = (1 - D)/4) run as the ladder (V_k, V_k+1, Q^k) with
 //        V_2k = V_k^2 - 2 Q^k,   V_2k+1 = V_k V_k+1 - P Q^k,
 //    the same four products for either exponent bit (the bit only selects operands), so the
@@ -45,58 +43,14 @@ __host__ __device__ __forceinline__ u64 inv64(u64 n)
     return x;
 }
 
-// the modulus with what the products need: 2n, n^-1 mod 2^64, -n^-1 mod 2^32, and R mod n
+// the modulus with what the products need: n^-1 mod 2^64 and R mod n
 struct Mod64 {
-    u64 n, n2;     // n and 2n (2n is used below 2^62 only)
+    u64 n;
     u64 ni;        // n^-1 mod 2^64 (the subtracting reduction)
     u64 one;       // R mod n, the residue of 1
-    u32 np;        // -n^-1 mod 2^32 (the adding reduction)
 };
 
-// ---- products: t = a b (128 bits), then one of the two reductions, result t / 2^64 ----
-
-// n < 2^62: every partial sum stays below 2^128 (a b < 4n^2 <= 2^126), so no carry word, and
-// the result (below 2n) is not reduced
-#define MM_REDUCE_LAZY                                   \
-    "mul.lo.u32     m, t0, %3;\n\t"                      \
-    "mad.lo.cc.u32  t0, m, n0, t0;\n\t"                  \
-    "madc.lo.cc.u32 t1, m, n1, t1;\n\t"                  \
-    "addc.cc.u32    t2, t2, 0;\n\t"                      \
-    "addc.u32       t3, t3, 0;\n\t"                      \
-    "mad.hi.cc.u32  t1, m, n0, t1;\n\t"                  \
-    "madc.hi.cc.u32 t2, m, n1, t2;\n\t"                  \
-    "addc.u32       t3, t3, 0;\n\t"                      \
-    "mul.lo.u32     m, t1, %3;\n\t"                      \
-    "mad.lo.cc.u32  t1, m, n0, t1;\n\t"                  \
-    "madc.lo.cc.u32 t2, m, n1, t2;\n\t"                  \
-    "addc.u32       t3, t3, 0;\n\t"                      \
-    "mad.hi.cc.u32  t2, m, n0, t2;\n\t"                  \
-    "madc.hi.u32    t3, m, n1, t3;\n\t"
-
-#define MM_REGS ".reg .u32 a0, a1, n0, n1, t0, t1, t2, t3, m;\n\t"
-
-// a^2 / R mod n by the lazy adding reduction, for n < 2^62: a in [0, 2n), result in [0, 2n)
-__device__ __forceinline__ u64 ml_sqr(u64 a, const Mod64 &M)
-{
-    u64 r;
-    asm("{\n\t" MM_REGS
-        "mov.b64 {a0, a1}, %1;\n\t"
-        "mov.b64 {n0, n1}, %2;\n\t"
-        "mul.lo.u32     t0, a0, a0;\n\t"
-        "mul.hi.u32     t1, a0, a0;\n\t"
-        "mul.lo.u32     t2, a1, a1;\n\t"
-        "mul.hi.u32     t3, a1, a1;\n\t"
-        "mad.lo.cc.u32  t1, a0, a1, t1;\n\t"
-        "madc.hi.cc.u32 t2, a0, a1, t2;\n\t"
-        "addc.u32       t3, t3, 0;\n\t"
-        "mad.lo.cc.u32  t1, a0, a1, t1;\n\t"
-        "madc.hi.cc.u32 t2, a0, a1, t2;\n\t"
-        "addc.u32       t3, t3, 0;\n\t"
-        MM_REDUCE_LAZY
-        "mov.b64 %0, {t2, t3};\n\t}"
-        : "=l"(r) : "l"(a), "l"(M.n), "r"(M.np));
-    return r;
-}
+// ---- products: t = a b (128 bits), then the reduction, result t / 2^64 ----
 
 // the subtracting reduction of t3:t2:t1:t0 (< n R): m = (t1:t0) n^-1 mod 2^64 (i1:i0), then
 // (t3:t2) - hi64(m n) + (n if it borrows).  The words of m n below 2^64 equal t1:t0, so only
@@ -173,28 +127,11 @@ __device__ __forceinline__ u64 ms_sqr(u64 a, const Mod64 &M)
     return r;
 }
 
-// x 2^b mod n for b in {0, 1}: a funnel shift by b, then one conditional subtraction.
-// LAZY (n < 2^62): x in [0, 2n), subtracts 2n, result in [0, 2n).  Otherwise x in [0, n), the
-// bit shifted out of 64 is kept, result in [0, n).
-template <bool LAZY>
+// x 2^b mod n for b in {0, 1} and x in [0, n): a funnel shift by b (the bit shifted out of 64
+// is kept), then one conditional subtraction; result in [0, n)
 __device__ __forceinline__ u64 mm_dbl(u64 x, u32 b, const Mod64 &M)
 {
     u64 r;
-    if (LAZY)
-        asm("{\n\t.reg .u32 x0, x1, n0, n1, y0, y1, d0, d1, bw;\n\t.reg .pred p;\n\t"
-            "mov.b64 {x0, x1}, %1;\n\t"
-            "mov.b64 {n0, n1}, %2;\n\t"
-            "shl.b32         y0, x0, %3;\n\t"
-            "shf.l.clamp.b32 y1, x0, x1, %3;\n\t"
-            "sub.cc.u32      d0, y0, n0;\n\t"
-            "subc.cc.u32     d1, y1, n1;\n\t"
-            "subc.u32        bw, 0, 0;\n\t"
-            "setp.ne.u32     p, bw, 0;\n\t"
-            "selp.u32        y0, y0, d0, p;\n\t"
-            "selp.u32        y1, y1, d1, p;\n\t"
-            "mov.b64 %0, {y0, y1};\n\t}"
-            : "=l"(r) : "l"(x), "l"(M.n2), "r"(b));
-    else
         asm("{\n\t.reg .u32 x0, x1, n0, n1, y0, y1, c, d0, d1, bw;\n\t.reg .pred p;\n\t"
             "mov.b64 {x0, x1}, %1;\n\t"
             "mov.b64 {n0, n1}, %2;\n\t"
@@ -227,21 +164,16 @@ __device__ __forceinline__ u64 mm_sub(u64 a, u64 b, u64 n)
     return a < b ? d + n : d;
 }
 
-// [0, 2n) -> [0, n)
-__device__ __forceinline__ u64 mm_canon(u64 x, u64 n) { return x >= n ? x - n : x; }
-
-// the modulus set-up: -n^-1 mod 2^32 and R mod n.  R mod n = 2^64 mod n is reached from
+// the modulus set-up: n^-1 mod 2^64 and R mod n.  R mod n = 2^64 mod n is reached from
 // 2^(bitlen(n) - 1) < n by doublings, which are exact.
 __device__ __forceinline__ Mod64 mm_setup(u64 n)
 {
     Mod64 M;
     M.n = n;
-    M.n2 = n << 1;
     M.ni = inv64(n);
-    M.np = 0u - (u32)M.ni;
     const int top = 63 - __clzll((long long)n);
     u64 x = 1ull << top;
-    for (int i = top; i < 64; i++) x = mm_dbl<false>(x, 1u, M);
+    for (int i = top; i < 64; i++) x = mm_dbl(x, 1u, M);
     M.one = x;
     return M;
 }
@@ -253,7 +185,7 @@ __device__ __forceinline__ u64 mm_from_small(i32 v, const Mod64 &M)
     const u32 a = v < 0 ? (u32)(-v) : (u32)v;
     u64 r = 0;
     for (int i = 31 - __clz(a | 1u); i >= 0; i--) {
-        r = mm_dbl<false>(r, 1u, M);
+        r = mm_dbl(r, 1u, M);
         if ((a >> i) & 1u) r = mm_add(r, M.one, M.n);
     }
     return (v < 0 && r) ? M.n - r : r;
@@ -261,13 +193,12 @@ __device__ __forceinline__ u64 mm_from_small(i32 v, const Mod64 &M)
 
 // ---- base-2 strong probable-prime test ----
 
-// size classes of the base-2 ladder: below 2^62 (lazy adding products), [2^62, 2^63) (the
-// doubling folded into a subtracting product), 2^63 and above (subtracting square, doubling)
-#define SP_LAZY 0
+// size classes of the base-2 ladder: below 2^63 (the doubling folded into the product), 2^63
+// and above (a square, then the doubling)
 #define SP_FOLD 1
 #define SP_WIDE 2
 
-__device__ __forceinline__ int spsp2_class(u64 n) { return n < (1ull << 62) ? SP_LAZY : n < (1ull << 63) ? SP_FOLD : SP_WIDE; }
+__device__ __forceinline__ int spsp2_class(u64 n) { return n < (1ull << 63) ? SP_FOLD : SP_WIDE; }
 
 // n - 1 = d 2^s with d odd: 2^d (mod n) by the left-to-right ladder, then the strong
 // condition 2^d = 1, or 2^(d 2^r) = -1 for some 0 <= r < s.  Odd n > 2 in size class CLS.
@@ -278,26 +209,21 @@ __device__ __forceinline__ bool spsp2(const Mod64 &M)
     const int s = __ffsll((long long)(n - 1)) - 1;
     const u64 d = (n - 1) >> s;
     const int L = 63 - __clzll((long long)d);               // d's top bit: the ladder starts at 2
-    u64 x = mm_dbl<false>(M.one, 1u, M);
+    u64 x = mm_dbl(M.one, 1u, M);
     for (int i = L - 1; i >= 0; i--) {
         const u32 bit = (u32)(d >> i) & 1u;
-        if (CLS == SP_LAZY) {
-            x = ml_sqr(x, M);
-            x = mm_dbl<true>(x, bit, M);
-        } else if (CLS == SP_FOLD) {
+        if (CLS == SP_FOLD) {
             x = ms_mul(x, x << bit, M);                     // x (x 2^bit) / R < 2 n^2 / R < n
         } else {
             x = ms_sqr(x, M);
-            x = mm_dbl<false>(x, bit, M);
+            x = mm_dbl(x, bit, M);
         }
     }
     const u64 mone = n - M.one;                             // the residue of -1
-    if (CLS == SP_LAZY) x = mm_canon(x, n);
     bool pass = x == M.one || x == mone;
     for (int r = 1; r < s && !pass; r++) {
         if (x == M.one) break;                              // 1 before -1: not a strong probable prime
-        if (CLS == SP_LAZY) x = mm_canon(ml_sqr(x, M), n);
-        else x = ms_sqr(x, M);
+        x = ms_sqr(x, M);
         pass = x == mone;
     }
     return pass;
@@ -308,7 +234,7 @@ __device__ __forceinline__ bool spsp2_u64(u64 n)
 {
     const Mod64 M = mm_setup(n);
     const int c = spsp2_class(n);
-    return c == SP_LAZY ? spsp2<SP_LAZY>(M) : c == SP_FOLD ? spsp2<SP_FOLD>(M) : spsp2<SP_WIDE>(M);
+    return c == SP_FOLD ? spsp2<SP_FOLD>(M) : spsp2<SP_WIDE>(M);
 }
 
 // ---- strong Lucas test ----
@@ -456,7 +382,7 @@ __device__ __forceinline__ bool bpsw_odd(u64 n)
     if (n == ~0ull) return false;
     const Mod64 M = mm_setup(n);
     const int c = spsp2_class(n);
-    const bool p2 = c == SP_LAZY ? spsp2<SP_LAZY>(M) : c == SP_FOLD ? spsp2<SP_FOLD>(M) : spsp2<SP_WIDE>(M);
+    const bool p2 = c == SP_FOLD ? spsp2<SP_FOLD>(M) : spsp2<SP_WIDE>(M);
     if (!p2) return false;
     const i32 D = selfridge_d(n);
     return D && lucas_strong(M, D);
