@@ -146,9 +146,10 @@ def _odd_part(x):
 TD_PRIMES = [3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37, 41, 43, 47, 53, 59, 61, 67, 71, 73, 79, 83, 89, 97, 101, 103,
              107, 109, 113, 127]
 # 32-bit multiply or multiply-add instructions (the multiply pipe) in one Montgomery product:
-# two limbs, 8 for the product and 10 for the two reduction rows (mp_mont64.cuh); three limbs
-# of the Fermat kernel, three rows of 3 + 3 (a b_i) + 1 (m) + 3 + 3 (m N) (mp_fermat.cu)
-IMAD_PER_PRODUCT_BPSW = 18
+# two limbs, 8 for the product, 4 for m = t n^-1 mod 2^64 and 7 for the high half of m n (the
+# subtracting reduction, mp_mont64.cuh); three limbs of the Fermat kernel, three rows of
+# 3 + 3 (a b_i) + 1 (m) + 3 + 3 (m N) (mp_fermat.cu)
+IMAD_PER_PRODUCT_BPSW = 19
 IMAD_PER_PRODUCT_FERMAT_K3 = 39
 
 
