@@ -71,6 +71,8 @@ extern "C" int mp_autotune(mp_handle *h, uint64_t lo, char *report, size_t cap)
         {"batched form", &h->tune.no_pipeline, {0, 1, 0}, 2, {"pipeline", "wave loop", ""}},
     };
     for (Knob &k : knobs) {
+        // the pipeline runs with the binned scatter only: with the staged one the knob changes nothing
+        if (k.field == &h->tune.no_pipeline && h->tune.scatter_staged) continue;
         float kb = 1e30f, k0 = 1e30f;
         int kv = k.vals[0];
         for (int i = 0; i < k.nv; i++) {
@@ -88,7 +90,7 @@ extern "C" int mp_autotune(mp_handle *h, uint64_t lo, char *report, size_t cap)
     h->tune_gen++;
     snprintf(line, sizeof line, "sieve choice: tile 2^%u, %u threads, %s scatter, bucket threshold tile/%d, %s\n", bt,
              bn, h->tune.scatter_staged ? "staged" : "binned", h->tune.bucket_div,
-             h->tune.no_pipeline ? "wave loop" : "pipeline");
+             (h->tune.no_pipeline || h->tune.scatter_staged) ? "wave loop" : "pipeline");
     rep += line;
     // Fermat: 2^20 primes near max(lo, 1e12), one vs two per thread
     u64 plo = std::max<u64>(lo, 1000000000000ull);
