@@ -4,8 +4,9 @@
 // test sprp2_64 :618 and the strong Lucas test slprp64 :766 with Selfridge's D :739), after
 // the trivial small-factor handling of is_prime_ref :529; the breadth-first batching of
 // test_batch64 :1392.  The arithmetic and the two tests are in mp_mont64.cuh.  Trial division
-// by the odd primes up to 127 uses the multiplicative-inverse test (q | n iff n q^-1 mod 2^64
-// <= (2^64 - 1) / q, for odd q), all 30 of them for every candidate, with no early exit.  The
+// by the odd primes up to 127 uses the multiplicative-inverse test (q | r iff r q^-1 mod 2^32
+// <= (2^32 - 1) / q, for odd q) on n's remainders modulo six products of them, all 30 primes
+// for every candidate, with no early exit.  The
 // verdict is primality for every n < 2^64 (BPSW has no pseudoprime below 2^64).
 //
 // Two launch structures:
@@ -26,19 +27,31 @@
 #include "mp_mont64.cuh"
 
 #define TD_N 30            // odd primes 3..127
+#define TD_NG 6            // in six groups whose products are below 2^32
 
-__constant__ u64 c_td_inv[TD_N];
-__constant__ u64 c_td_lim[TD_N];
+__constant__ u32 c_tdg_prod[TD_NG];      // the groups' products
+__constant__ u64 c_tdg_magic[TD_NG];     // floor((2^64 - 1) / product), for the Barrett remainder
+__constant__ u32 c_td_inv32[TD_N];       // p^-1 mod 2^32
+__constant__ u32 c_td_lim32[TD_N];       // floor((2^32 - 1) / p)
 __constant__ u64 c_small_prime_mask[2];   // bit n set iff n < 128 is prime
 
 // ---- trial division ----
-// 1 = prime, 0 = composite, -1 = undecided (odd, no factor <= 127, n >= 131^2)
+// 1 = prime, 0 = composite, -1 = undecided (odd, no factor <= 127, n >= 131^2).  Per group one
+// 64-bit Barrett remainder r = n mod (product of the group), then for each prime p of the group
+// p | r iff r p^-1 mod 2^32 <= (2^32 - 1) / p: one 32-bit multiply and one compare a prime,
+// instead of a 64-bit product and a 64-bit compare
 __device__ __forceinline__ int td_verdict(u64 n)
 {
     if (n < 128) return (int)((c_small_prime_mask[n >> 6] >> (n & 63)) & 1);
     bool f = !(n & 1);
+    const int gsize[TD_NG] = {8, 5, 5, 5, 4, 3};   // 3..23, 29..43, 47..67, 71..89, 97..107, 109..127
+    int k = 0;
 #pragma unroll
-    for (int k = 0; k < TD_N; k++) f |= n * c_td_inv[k] <= c_td_lim[k];
+    for (int g = 0; g < TD_NG; g++) {
+        const u32 r = mp_mod_barrett(n, c_tdg_prod[g], c_tdg_magic[g]);
+#pragma unroll
+        for (int j = 0; j < gsize[g]; j++, k++) f |= r * c_td_inv32[k] <= c_td_lim32[k];
+    }
     if (f) return 0;
     return n < 131ull * 131ull ? 1 : -1;
 }
@@ -203,19 +216,30 @@ static int bpsw_consts(mp_handle *h)
     if (h->device >= 0 && h->device < 16 && g_bpsw_consts[h->device]) return MP_OK;
     static const u32 tdp[TD_N] = {3,  5,  7,  11, 13, 17, 19, 23, 29, 31, 37, 41,  43,  47,  53,
                                   59, 61, 67, 71, 73, 79, 83, 89, 97, 101, 103, 107, 109, 113, 127};
-    u64 inv[TD_N], lim[TD_N], mask[2] = {0, 0};
+    static const int gsize[TD_NG] = {8, 5, 5, 5, 4, 3};
+    u32 inv[TD_N], lim[TD_N], prod[TD_NG];
+    u64 magic[TD_NG], mask[2] = {0, 0};
     for (int k = 0; k < TD_N; k++) {
-        const u64 q = tdp[k];
-        inv[k] = inv64(q);
-        lim[k] = ~0ull / q;
+        const u32 q = tdp[k];
+        inv[k] = (u32)inv64(q);              // q^-1 mod 2^64, so also mod 2^32
+        lim[k] = 0xffffffffu / q;
+    }
+    for (int g = 0, k = 0; g < TD_NG; g++) {
+        u64 pr = 1;
+        for (int j = 0; j < gsize[g]; j++, k++) pr *= tdp[k];
+        if (pr >> 32) return mp_set_error(h, MP_EINVAL, "trial-division group product above 2^32");
+        prod[g] = (u32)pr;
+        magic[g] = ~0ull / pr;
     }
     for (u32 v = 2; v < 128; v++) {
         bool p = true;
         for (u32 d = 2; d * d <= v; d++) if (v % d == 0) { p = false; break; }
         if (p) mask[v >> 6] |= 1ull << (v & 63);
     }
-    MP_CUDA(h, cudaMemcpyToSymbol(c_td_inv, inv, sizeof inv));
-    MP_CUDA(h, cudaMemcpyToSymbol(c_td_lim, lim, sizeof lim));
+    MP_CUDA(h, cudaMemcpyToSymbol(c_td_inv32, inv, sizeof inv));
+    MP_CUDA(h, cudaMemcpyToSymbol(c_td_lim32, lim, sizeof lim));
+    MP_CUDA(h, cudaMemcpyToSymbol(c_tdg_prod, prod, sizeof prod));
+    MP_CUDA(h, cudaMemcpyToSymbol(c_tdg_magic, magic, sizeof magic));
     MP_CUDA(h, cudaMemcpyToSymbol(c_small_prime_mask, mask, sizeof mask));
     if (h->device >= 0 && h->device < 16) g_bpsw_consts[h->device] = true;
     return MP_OK;
