@@ -106,24 +106,29 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def algorithmic_work(primes, lo, hi, tile_bits):
-    """Exact marks of the sieve: the multiples m = k q of each sieving prime q >= 97 with k
-    coprime to 30 (the wheel of 30; the presieve patterns mark the multiples of 3 and 5) and
-    max(lo, q^2) <= m < hi + tail, split at the tile size: marks by primes q <= tile_bits are
-    shared-memory atomics, those above are bucket records (4 bytes written + 4 read)."""
+def algorithmic_work(primes, lo, hi, tile_bits, staged=True):
+    """Exact marks of the sieve: the multiples m = k q of each sieving prime q >= 97 with
+    max(lo, q^2) <= m < hi + tail, split at the tile size.  Primes q <= tile_bits mark the k
+    coprime to 30 (the wheel of 30; the presieve patterns mark the multiples of 3 and 5) with
+    shared-memory atomics; larger primes write a bucket record (4 bytes written + 4 read) for the
+    k coprime to 210 (the staged scatter's wheel of 210: the patterns mark the multiples of 7 too);
+    with the binned scatter (staged=False) the bucket primes keep the wheel of 30."""
     qi = primes[primes >= 97].astype(np.uint64)
     top = hi + (1 << 16)
     start = np.maximum(np.full(len(qi), lo, dtype=np.uint64), qi * qi)
-    below = np.array([sum(1 for r in (1, 7, 11, 13, 17, 19, 23, 29) if r < x) for x in range(30)], dtype=np.uint64)
-
-    def coprime_below(k):                          # k' < k with gcd(k', 30) = 1
-        return np.uint64(8) * (k // np.uint64(30)) + below[(k % np.uint64(30)).astype(np.int64)]
-
     k0 = (start + qi - np.uint64(1)) // qi         # first k with k q >= start
     k1 = np.maximum((np.uint64(top) + qi - np.uint64(1)) // qi, k0)
-    m = (coprime_below(k1) - coprime_below(k0)).astype(np.float64)
+
+    def coprime_below(k, wheel):                   # k' < k with gcd(k', wheel) = 1
+        res = [r for r in range(wheel) if np.gcd(r, wheel) == 1]
+        below = np.array([sum(1 for r in res if r < x) for x in range(wheel)], dtype=np.uint64)
+        return np.uint64(len(res)) * (k // np.uint64(wheel)) + below[(k % np.uint64(wheel)).astype(np.int64)]
+
     small = qi <= np.uint64(tile_bits)
-    return float(m[small].sum()), float(m[~small].sum())
+    wheel = 210 if staged else 30
+    m30 = (coprime_below(k1[small], 30) - coprime_below(k0[small], 30)).astype(np.float64)
+    mb = (coprime_below(k1[~small], wheel) - coprime_below(k0[~small], wheel)).astype(np.float64)
+    return float(m30.sum()), float(mb.sum())
 
 
 def _bitlen64(x):
@@ -358,8 +363,9 @@ def run_ours(args):
             tile_bits = 1 << int(m.group(1))
         m = re.search(r"bucket threshold tile/(\d+)", tune_report.split("sieve choice")[-1])
         bucket_div = int(m.group(1)) if m else 1
-        marks_small, marks_large = algorithmic_work(primes, lo, hi, tile_bits // bucket_div)
         ntiles = -(-((hi + (1 << 16) - lo) // 2) // tile_bits)
+        staged = "binned scatter" not in tune_report.split("sieve choice")[-1]
+        marks_small, marks_large = algorithmic_work(primes, lo, hi, tile_bits // bucket_div, staged)
         pipe_launches, pipe_ms = prof.get("pipeline", (0, 0.0))
         if pipe_launches:
             # one persistent launch per step runs the scatter and the tiles: its bytes are the

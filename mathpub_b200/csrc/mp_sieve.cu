@@ -615,8 +615,9 @@ struct ScatterArgs {
 // Every hit j of a large prime q in the wave (plus the first HALO_BITS bits after it) is a
 // record (tile, offset) of its own tile, and also (tile - 1, offset + 2^TLOG) when it lies in
 // the first HALO_BITS bits of a tile, because the previous tile sieves those bits as its halo.
-// The hits are the multiples q k with k coprime to 30 (the wheel of 30): 8 progressions of
-// stride 15 q.
+// The staged scatter's hits are the multiples q k with k coprime to 210 (the wheel of 210, below:
+// 48 progressions of stride 105 q, walked eight at a time); the binned scatter's are those with k
+// coprime to 30 (the wheel of 30: 8 progressions of stride 15 q).
 //
 // One pass, staged in shared memory: each persistent CTA owns a run of primes of equal sum
 // of 1/q (equal expected hits); every thread walks one prime at a time, one turn of the wheel
@@ -659,6 +660,98 @@ __device__ __forceinline__ bool scatter_setup(const ScatterArgs &a, u32 k, u64 x
         jj[i] = j < span ? (u32)j : span;
         j += (u64)q * (s & 3u);
         s >>= 2;
+    }
+    return jj[0] < span;
+}
+
+// The staged scatter walks the wheel of 210: a bucket prime q marks only the q k with k coprime
+// to 210, the multiples of 7 among the wheel-30 hits being marked by the presieve patterns
+// already (1/7 of the records fewer).  The 48 residues of k mod 210 (all odd) give 48
+// progressions of stride 105 q bits; a thread walks them eight at a time, as six groups.
+// c_w210_off[t] = (R[t mod 48] + 210 (t div 48) - 1) / 2 for the residues R in increasing
+// order, so the progression m places from residue index w lies q (off[w + m] - off[w]) bits on;
+// for an odd k mod 210, c_w210_nidx / c_w210_ndist give the index of the first residue at or
+// above it and the distance to it in q bits; c_w210_inv[q mod 210] = q^-1 mod 210.
+__constant__ u8 c_w210_off[96] = {
+    0, 5, 6, 8, 9, 11, 14, 15, 18, 20, 21, 23, 26, 29, 30, 33, 35, 36, 39, 41, 44, 48, 50, 51,
+    53, 54, 56, 60, 63, 65, 68, 69, 71, 74, 75, 78, 81, 83, 84, 86, 89, 90, 93, 95, 96, 98, 99, 104,
+    105, 110, 111, 113, 114, 116, 119, 120, 123, 125, 126, 128, 131, 134, 135, 138, 140, 141, 144, 146, 149, 153, 155, 156,
+    158, 159, 161, 165, 168, 170, 173, 174, 176, 179, 180, 183, 186, 188, 189, 191, 194, 195, 198, 200, 201, 203, 204, 209,
+};
+__constant__ u8 c_w210_nidx[210] = {
+    0, 0, 0, 1, 0, 1, 0, 1, 0, 1, 0, 1, 0, 2, 0, 3, 0, 3, 0, 4, 0, 5, 0, 5,
+    0, 6, 0, 6, 0, 6, 0, 7, 0, 8, 0, 8, 0, 8, 0, 9, 0, 9, 0, 10, 0, 11, 0, 11,
+    0, 12, 0, 12, 0, 12, 0, 13, 0, 13, 0, 13, 0, 14, 0, 15, 0, 15, 0, 15, 0, 16, 0, 16,
+    0, 17, 0, 18, 0, 18, 0, 18, 0, 19, 0, 19, 0, 20, 0, 20, 0, 20, 0, 21, 0, 21, 0, 21,
+    0, 21, 0, 22, 0, 22, 0, 23, 0, 24, 0, 24, 0, 25, 0, 26, 0, 26, 0, 27, 0, 27, 0, 27,
+    0, 27, 0, 28, 0, 28, 0, 28, 0, 29, 0, 29, 0, 30, 0, 30, 0, 30, 0, 31, 0, 32, 0, 32,
+    0, 33, 0, 33, 0, 33, 0, 34, 0, 35, 0, 35, 0, 35, 0, 36, 0, 36, 0, 36, 0, 37, 0, 37,
+    0, 38, 0, 39, 0, 39, 0, 40, 0, 40, 0, 40, 0, 41, 0, 42, 0, 42, 0, 42, 0, 43, 0, 43,
+    0, 44, 0, 45, 0, 45, 0, 46, 0, 47, 0, 47, 0, 47, 0, 47, 0, 47,
+};
+__constant__ u8 c_w210_ndist[210] = {
+    0, 0, 0, 4, 0, 3, 0, 2, 0, 1, 0, 0, 0, 0, 0, 1, 0, 0, 0, 0, 0, 1, 0, 0,
+    0, 2, 0, 1, 0, 0, 0, 0, 0, 2, 0, 1, 0, 0, 0, 1, 0, 0, 0, 0, 0, 1, 0, 0,
+    0, 2, 0, 1, 0, 0, 0, 2, 0, 1, 0, 0, 0, 0, 0, 2, 0, 1, 0, 0, 0, 1, 0, 0,
+    0, 0, 0, 2, 0, 1, 0, 0, 0, 1, 0, 0, 0, 2, 0, 1, 0, 0, 0, 3, 0, 2, 0, 1,
+    0, 0, 0, 1, 0, 0, 0, 0, 0, 1, 0, 0, 0, 0, 0, 1, 0, 0, 0, 3, 0, 2, 0, 1,
+    0, 0, 0, 2, 0, 1, 0, 0, 0, 1, 0, 0, 0, 2, 0, 1, 0, 0, 0, 0, 0, 1, 0, 0,
+    0, 2, 0, 1, 0, 0, 0, 0, 0, 2, 0, 1, 0, 0, 0, 2, 0, 1, 0, 0, 0, 1, 0, 0,
+    0, 0, 0, 1, 0, 0, 0, 2, 0, 1, 0, 0, 0, 0, 0, 2, 0, 1, 0, 0, 0, 1, 0, 0,
+    0, 0, 0, 1, 0, 0, 0, 0, 0, 4, 0, 3, 0, 2, 0, 1, 0, 0,
+};
+__constant__ u8 c_w210_inv[210] = {
+    0, 1, 0, 0, 0, 0, 0, 0, 0, 0, 0, 191, 0, 97, 0, 0, 0, 173, 0, 199, 0, 0, 0, 137,
+    0, 0, 0, 0, 0, 29, 0, 61, 0, 0, 0, 0, 0, 193, 0, 0, 0, 41, 0, 127, 0, 0, 0, 143,
+    0, 0, 0, 0, 0, 107, 0, 0, 0, 0, 0, 89, 0, 31, 0, 0, 0, 0, 0, 163, 0, 0, 0, 71,
+    0, 187, 0, 0, 0, 0, 0, 109, 0, 0, 0, 167, 0, 0, 0, 0, 0, 59, 0, 0, 0, 0, 0, 0,
+    0, 13, 0, 0, 0, 131, 0, 157, 0, 0, 0, 53, 0, 79, 0, 0, 0, 197, 0, 0, 0, 0, 0, 0,
+    0, 151, 0, 0, 0, 0, 0, 43, 0, 0, 0, 101, 0, 0, 0, 0, 0, 23, 0, 139, 0, 0, 0, 47,
+    0, 0, 0, 0, 0, 179, 0, 121, 0, 0, 0, 0, 0, 103, 0, 0, 0, 0, 0, 67, 0, 0, 0, 83,
+    0, 169, 0, 0, 0, 17, 0, 0, 0, 0, 0, 149, 0, 181, 0, 0, 0, 0, 0, 73, 0, 0, 0, 11,
+    0, 37, 0, 0, 0, 113, 0, 19, 0, 0, 0, 0, 0, 0, 0, 0, 0, 209,
+};
+
+struct W210 {                                    // the tables, staged in shared memory per CTA
+    u8 off[96], nidx[210], ndist[210], inv[210];
+};
+
+__device__ __forceinline__ void w210_load(W210 &t)
+{
+    for (u32 i = threadIdx.x; i < 210; i += blockDim.x) {
+        if (i < 96) t.off[i] = c_w210_off[i];
+        t.nidx[i] = c_w210_nidx[i];
+        t.ndist[i] = c_w210_ndist[i];
+        t.inv[i] = c_w210_inv[i];
+    }
+}
+
+// prime k over the wave: the bit jf of its first hit (a multiple q k' >= max(x0, q^2) with k'
+// coprime to 210) and the residue index w of k'; false when the wave has none.  xm = x0 mod 210
+__device__ __forceinline__ bool w210_prime(const ScatterArgs &a, const W210 &t, u32 k, u64 x0, u32 xm, u32 span,
+                                           u32 &q, u32 &jf, u32 &w)
+{
+    q = __ldg(a.q + k);
+    const u32 r = mp_mod_barrett(x0, q, __ldg(a.magic + k));
+    const u64 j64 = mp_first_odd_multiple(x0, q, r, span);
+    if (j64 >= span) return false;
+    const u32 km = (xm + 2u * (u32)(j64 % 105u)) % 210u * t.inv[q % 210u] % 210u;   // k mod 210
+    w = t.nidx[km];
+    const u64 j = j64 + (u64)q * t.ndist[km];
+    if (j >= span) return false;
+    jf = (u32)j;
+    return true;
+}
+
+// group g (0..5) of the prime: the starts of its eight progressions, ascending, below the
+// first one + 105 q (or span when past the wave's end); false when the group has no hit
+__device__ __forceinline__ bool w210_group(const W210 &t, u32 q, u32 jf, u32 w, u32 g, u32 span, u32 *jj)
+{
+    const u32 b = t.off[w];
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        const u64 j = jf + (u64)q * (u32)(t.off[w + 8 * g + i] - b);
+        jj[i] = j < span ? (u32)j : span;
     }
     return jj[0] < span;
 }
@@ -730,26 +823,47 @@ __global__ void __launch_bounds__(SC_THREADS, SC_CTAS_PER_SM) scatter_kernel(Sca
     u32 *stage = ssm, *sorted = ssm + SC_STAGE, *hist = ssm + 2 * SC_STAGE, *gb = hist + a.wt;
     __shared__ u32 s_fill;
     __shared__ u32 s_wsum[SC_THREADS / 32];
+    __shared__ W210 s_w210;
     const u32 tid = threadIdx.x, lane = tid & 31, wt = a.wt, tlog = a.tlog, tmask = (1u << tlog) - 1;
     for (u32 i = tid; i < wt; i += SC_THREADS) hist[i] = 0;
     if (tid == 0) s_fill = 0;
+    w210_load(s_w210);
     const u64 wstart = (u64)a.t0 << tlog;
     u64 wend = (u64)(a.t0 + wt) << tlog;
     if (wend > a.nbx) wend = a.nbx;
     u64 wend_halo = wend + HALO_BITS;
     if (wend_halo > a.nbx) wend_halo = a.nbx;
     const u64 x0 = a.base + 2 * wstart + 1;
-    const u32 xm = (u32)(x0 % 30u);
+    const u32 xm = (u32)(x0 % 210u);
     const u32 span = (u32)(wend_halo - wstart);          // < 2^31 (checked by the planner)
     const u32 k1 = __ldg(a.bounds + blockIdx.x + 1);
     u32 k = __ldg(a.bounds + blockIdx.x) + tid;
-    u32 jj[8], turn = 0;
+    // the thread's prime q, its first hit jf and residue index w, and the group g of its eight
+    // progressions being walked (5: no group left)
+    u32 jj[8], turn = 0, q = 0, jf = 0, w = 0, g = 5;
     bool have = false;
     __syncthreads();
     for (;;) {
-        while (!have && k < k1) {
-            have = scatter_setup(a, k, x0, xm, span, jj, turn);
-            k += SC_THREADS;
+        while (!have) {
+            if (g < 5) {
+                // the next group; groups start further on one after the other, so a group with no
+                // hit ends the prime
+                have = w210_group(s_w210, q, jf, w, ++g, span, jj);
+                if (!have) g = 5;
+            } else if (k < k1) {
+                if (w210_prime(a, s_w210, k, x0, xm, span, q, jf, w)) {
+                    // span < 2^31: a stride of 2^31 or more leaves one hit per progression at
+                    // most, so it is clamped there and the positions stay below 2^32
+                    const u64 turn64 = 105ull * q;
+                    turn = turn64 >= (1ull << 31) ? (1u << 31) : (u32)turn64;
+                    g = 0;
+                    have = w210_group(s_w210, q, jf, w, 0, span, jj);
+                    if (!have) g = 5;
+                }
+                k += SC_THREADS;
+            } else {
+                break;
+            }
         }
         if (!__syncthreads_or(have)) break;                // the last round's appends are done
         // every thread takes the fill before any thread appends again, so the flush decision
