@@ -43,7 +43,8 @@ HASH_LOG2 = 20
 BPSW_SEED, BPSW_COUNT, BPSW_LISTS = 0x3C0FFEE, 1 << 26, 4096
 HBM_FALLBACK_GBS = 6650.0
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one tile-kernel launch (a wave
-# of 1184 tiles at 1e15), from an ncu capture of that launch
+# of 1184 tiles at 1e15), from an ncu capture of that launch, taken while the bucket records
+# were still on the wheel of 30 (1.006e9 a step; the wheel of 210 writes 8.63e8)
 TILE_TRAFFIC_BYTES = 597.9e6 + 297.7e6
 # the same for the persistent pipeline launch of one step (None until captured)
 PIPE_TRAFFIC_BYTES = None
@@ -380,8 +381,9 @@ def run_ours(args):
             kbytes = (marks_large * 4 + ntiles * (tile_bits // 8)) / max(tile_launches, 1)
             ktraffic = TILE_TRAFFIC_BYTES
             knote = ("bytes = bucket records read (4 B per large-prime hit) + bitmap written; traffic = DRAM bytes of "
-                     "one launch from an ncu capture; the kernel is bound by instruction issue and shared-memory "
-                     "atomics, see roofline_smem")
+                     "one launch from an ncu capture taken with the bucket records on the wheel of 30 (14% more "
+                     "records than this build's wheel of 210); the kernel is bound by instruction issue and "
+                     "shared-memory atomics, see roofline_smem")
         tile_avg_s = kms / max(klaunches, 1) / 1e3
         achieved = kbytes / tile_avg_s / 1e9
         smem_marks_rate = (marks_small + marks_large) / (kms / 1e3)
